@@ -1,0 +1,423 @@
+// Astrocyte-only engine: the drop-in for the reference's native CUDA
+// astrocyte backend (astrocyte_cuda.hpp:15-27, astrocyte_cuda.cu:27-155) and
+// the astrocyte kernel-scaling workload with its input generated on the
+// device.
+//
+// Layout: SoA FP64 arrays Ca, IP3, h (+ Ca_tot, IP3_0, tau_IP3, delta_IP3
+// when per-cell), 256-byte aligned.  Each thread owns two adjacent cells so
+// every state array is read and written with one coalesced 128-bit access
+// per thread, and the two independent RK4 chains interleave to cover FP64
+// latency.  Grid-stride loop over cell pairs; grid sized in multiples of
+// the SM count.
+//
+// Compiled with -fmad=false: results are bitwise equal to the host's
+// astro_advance (no transcendental on this path when noise is off).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "asg_common.hpp"
+#include "asg_device.cuh"
+
+namespace asg {
+
+namespace {
+
+struct AstroArrays {
+    double* Ca;
+    double* IP3;
+    double* h;
+    double* input;  // per-step input (drop-in path) or nullptr
+    const double* Ca_tot;
+    const double* IP3_0;
+    const double* tau;
+    const double* delta;
+};
+
+struct UniformParams {
+    double Ca_tot, IP3_0, tau, delta;
+};
+
+enum InputMode { kInputArray = 0, kInputBernoulli = 1 };
+
+struct StepArgs {
+    std::int64_t n;
+    AstroK k;
+    UniformParams u;
+    // noise (drop-in path)
+    double noise_std;
+    int independent;
+    double shared_noise;
+    std::uint64_t noise_seed, noise_index;
+    // Bernoulli input (scaling path)
+    std::uint64_t seed;
+    double p, weight;
+    const std::int64_t* step_base;  // device counter: step = *step_base + step_offset
+    int step_offset;
+};
+
+template <bool kUniform, int kInput, bool kNoise>
+__device__ __forceinline__ void advance_cell(const StepArgs& a, const AstroArrays& s,
+                                             std::int64_t i, std::int64_t step, double& ca,
+                                             double& ip3, double& hh) {
+    double in;
+    if (kInput == kInputBernoulli) {
+        in = uniform_at(a.seed, static_cast<std::uint64_t>(i),
+                        1000ULL + static_cast<std::uint64_t>(step)) < a.p
+                 ? a.weight
+                 : 0.0;
+    } else {
+        in = s.input[i];
+    }
+    double noise = 0.0;
+    if (kNoise) {
+        noise = a.independent
+                    ? a.noise_std * normal_clamped(a.noise_seed, a.noise_index * kStreamStride +
+                                                                     static_cast<std::uint64_t>(i))
+                    : a.shared_noise;
+    }
+    if (kUniform) {
+        astro_rk4(a.k, a.u.Ca_tot, a.u.IP3_0, a.u.tau, a.u.delta, in, noise, ca, ip3, hh);
+    } else {
+        astro_rk4(a.k, s.Ca_tot[i], s.IP3_0[i], s.tau[i], s.delta[i], in, noise, ca, ip3, hh);
+    }
+}
+
+template <bool kUniform, int kInput, bool kNoise>
+__global__ void __launch_bounds__(128, 4) astro_step_kernel(StepArgs a, AstroArrays s) {
+    const std::int64_t step =
+        (kInput == kInputBernoulli) ? (*a.step_base + a.step_offset) : 0;
+    const std::int64_t pairs = a.n / 2;
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    double2* Ca2 = reinterpret_cast<double2*>(s.Ca);
+    double2* IP32 = reinterpret_cast<double2*>(s.IP3);
+    double2* h2 = reinterpret_cast<double2*>(s.h);
+    for (std::int64_t p = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+         p < pairs; p += stride) {
+        double2 ca = Ca2[p], ip3 = IP32[p], hh = h2[p];
+        const std::int64_t i = 2 * p;
+        advance_cell<kUniform, kInput, kNoise>(a, s, i, step, ca.x, ip3.x, hh.x);
+        advance_cell<kUniform, kInput, kNoise>(a, s, i + 1, step, ca.y, ip3.y, hh.y);
+        Ca2[p] = ca;
+        IP32[p] = ip3;
+        h2[p] = hh;
+        if (kInput == kInputArray) reinterpret_cast<double2*>(s.input)[p] = make_double2(0.0, 0.0);
+    }
+    // Odd tail cell.
+    if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const std::int64_t i = a.n - 1;
+        double ca = s.Ca[i], ip3 = s.IP3[i], hh = s.h[i];
+        advance_cell<kUniform, kInput, kNoise>(a, s, i, step, ca, ip3, hh);
+        s.Ca[i] = ca;
+        s.IP3[i] = ip3;
+        s.h[i] = hh;
+        if (kInput == kInputArray) s.input[i] = 0.0;
+    }
+}
+
+__global__ void advance_counter_kernel(std::int64_t* base, std::int64_t by) { *base += by; }
+
+AstroK make_astro_k(const double* c, double h_step, int substeps) {
+    // c: Kd_IP3_1, Kd_IP3_2, Kd_act, Kd_inh, Km_SERCA, k_IP3R, rate_IP3R,
+    //    rate_L, rate_SERCA, ratio_ER_cyt
+    AstroK k{};
+    k.Kd_IP3_1 = c[0];
+    k.Kd_IP3_2 = c[1];
+    k.Kd_act = c[2];
+    k.ratio_ER_cyt = c[9];
+    k.chan = c[9] * c[6];
+    k.serca = c[8];
+    k.km2 = c[4] * c[4];
+    k.leak = c[9] * c[7];
+    k.ah = c[5] * c[3];
+    k.k_IP3R = c[5];
+    k.half_h = 0.5 * h_step;
+    k.h = h_step;
+    k.h6 = h_step / 6.0;
+    k.substeps = substeps;
+    return k;
+}
+
+}  // namespace
+
+struct AstroEngine {
+    std::int64_t n = 0;
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevBuf Ca, IP3, h, input, Ca_tot, IP3_0, tau, delta, step_base;
+    double last_ms = 0.0;
+    std::int64_t last_kernels = 0;
+    // Captured chunk of Bernoulli steps, rebuilt when its arguments change.
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    StepArgs graph_args{};
+    bool graph_uniform = true;
+
+    ~AstroEngine() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    int grid_for(std::int64_t pairs, int block) const {
+        const std::int64_t want = (pairs + block - 1) / block;
+        const std::int64_t cap = static_cast<std::int64_t>(sms) * 16;
+        return static_cast<int>(std::max<std::int64_t>(1, std::min(want, cap)));
+    }
+
+    AstroArrays arrays() {
+        return AstroArrays{Ca.as<double>(),        IP3.as<double>(),       h.as<double>(),
+                           input.as<double>(),     Ca_tot.as<double>(),    IP3_0.as<double>(),
+                           tau.as<double>(),       delta.as<double>()};
+    }
+};
+
+}  // namespace asg
+
+using asg::AstroEngine;
+
+extern "C" {
+
+int asg_astro_create(uint32_t n, const double* Ca, const double* IP3, const double* h,
+                     const double* Ca_tot, const double* IP3_0, const double* tau_IP3,
+                     const double* delta_IP3, asg_astro** out) {
+    asg::clear_error();
+    if (out == nullptr) return asg::fail(ASG_ERR_ARG, "asg_astro_create: out is NULL");
+    *out = nullptr;
+    if (n > 0 && (Ca == nullptr || IP3 == nullptr || h == nullptr))
+        return asg::fail(ASG_ERR_ARG, "asg_astro_create: state arrays are required");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return asg::fail(ASG_ERR_NO_DEVICE, "asg_astro_create: no CUDA device");
+    auto* e = new AstroEngine;
+    e->n = n;
+    cudaGetDevice(&e->device);
+    cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->device);
+    const std::size_t bytes = static_cast<std::size_t>(n) * sizeof(double);
+    int st = ASG_OK;
+    // Parameter arrays are optional (the scaling run takes uniform scalars);
+    // a NULL parameter array allocates nothing.
+    auto upload = [&](asg::DevBuf& b, const double* src, bool required) {
+        if (st != ASG_OK || (src == nullptr && !required)) return;
+        st = b.alloc(bytes, src == nullptr);
+        if (st == ASG_OK && src != nullptr && bytes > 0) {
+            const cudaError_t ce = cudaMemcpy(b.get(), src, bytes, cudaMemcpyHostToDevice);
+            if (ce != cudaSuccess) st = asg::cuda_fail(ce, "upload", __FILE__, __LINE__);
+        }
+    };
+    upload(e->Ca, Ca, true);
+    upload(e->IP3, IP3, true);
+    upload(e->h, h, true);
+    upload(e->input, nullptr, true);
+    upload(e->Ca_tot, Ca_tot, false);
+    upload(e->IP3_0, IP3_0, false);
+    upload(e->tau, tau_IP3, false);
+    upload(e->delta, delta_IP3, false);
+    if (st == ASG_OK) st = e->step_base.alloc(sizeof(std::int64_t));
+    if (st == ASG_OK) {
+        cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+        if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev0);
+        if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev1);
+        if (ce != cudaSuccess) st = asg::cuda_fail(ce, "stream/event", __FILE__, __LINE__);
+    }
+    if (st != ASG_OK) {
+        delete e;
+        return st;
+    }
+    *out = reinterpret_cast<asg_astro*>(e);
+    return ASG_OK;
+}
+
+int asg_astro_destroy(asg_astro* s, double* Ca, double* IP3, double* h) {
+    asg::clear_error();
+    if (s == nullptr) return ASG_OK;
+    auto* e = reinterpret_cast<AstroEngine*>(s);
+    int st = ASG_OK;
+    if (e->n > 0 && Ca != nullptr && IP3 != nullptr && h != nullptr) {
+        st = asg_astro_pull_state(s, Ca, IP3, h);
+    }
+    delete e;
+    return st;
+}
+
+int asg_astro_pull_state(asg_astro* s, double* Ca, double* IP3, double* h) {
+    asg::clear_error();
+    if (s == nullptr) return asg::fail(ASG_ERR_ARG, "asg_astro_pull_state: NULL handle");
+    auto* e = reinterpret_cast<AstroEngine*>(s);
+    const std::size_t bytes = static_cast<std::size_t>(e->n) * sizeof(double);
+    if (bytes == 0) return ASG_OK;
+    ASG_CUDA(cudaMemcpyAsync(Ca, e->Ca.get(), bytes, cudaMemcpyDeviceToHost, e->stream));
+    ASG_CUDA(cudaMemcpyAsync(IP3, e->IP3.get(), bytes, cudaMemcpyDeviceToHost, e->stream));
+    ASG_CUDA(cudaMemcpyAsync(h, e->h.get(), bytes, cudaMemcpyDeviceToHost, e->stream));
+    ASG_CUDA(cudaStreamSynchronize(e->stream));
+    return ASG_OK;
+}
+
+int asg_astro_push_input(asg_astro* s, const double* ip3_input) {
+    asg::clear_error();
+    if (s == nullptr || ip3_input == nullptr)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_push_input: NULL argument");
+    auto* e = reinterpret_cast<AstroEngine*>(s);
+    const std::size_t bytes = static_cast<std::size_t>(e->n) * sizeof(double);
+    if (bytes == 0) return ASG_OK;
+    ASG_CUDA(cudaMemcpyAsync(e->input.get(), ip3_input, bytes, cudaMemcpyHostToDevice,
+                             e->stream));
+    return ASG_OK;
+}
+
+int asg_astro_pull_calcium(asg_astro* s, double* Ca) {
+    asg::clear_error();
+    if (s == nullptr || Ca == nullptr)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_pull_calcium: NULL argument");
+    auto* e = reinterpret_cast<AstroEngine*>(s);
+    const std::size_t bytes = static_cast<std::size_t>(e->n) * sizeof(double);
+    if (bytes == 0) return ASG_OK;
+    ASG_CUDA(cudaMemcpyAsync(Ca, e->Ca.get(), bytes, cudaMemcpyDeviceToHost, e->stream));
+    ASG_CUDA(cudaStreamSynchronize(e->stream));
+    return ASG_OK;
+}
+
+int asg_astro_update(asg_astro* s, const double* consts, double h_step, int32_t substeps,
+                     double noise_std, int32_t independent_noise, double shared_noise,
+                     uint64_t noise_seed, uint64_t noise_index) {
+    asg::clear_error();
+    if (s == nullptr || consts == nullptr)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_update: NULL argument");
+    if (substeps < 0) return asg::fail(ASG_ERR_ARG, "asg_astro_update: substeps < 0");
+    auto* e = reinterpret_cast<AstroEngine*>(s);
+    if (e->n == 0) return ASG_OK;
+    if (e->Ca_tot.get() == nullptr) {
+        return asg::fail(ASG_ERR_STATE,
+                         "asg_astro_update: per-cell parameters were not given at create");
+    }
+    asg::StepArgs a{};
+    a.n = e->n;
+    a.k = asg::make_astro_k(consts, h_step, substeps);
+    a.noise_std = noise_std;
+    a.independent = independent_noise;
+    a.shared_noise = shared_noise;
+    a.noise_seed = noise_seed;
+    a.noise_index = noise_index;
+    a.step_base = e->step_base.as<std::int64_t>();
+    const int block = 128;
+    const int grid = e->grid_for(std::max<std::int64_t>(1, e->n / 2), block);
+    ASG_CUDA(cudaEventRecord(e->ev0, e->stream));
+    // The reference applies noise only when noise_std > 0 (astrocyte.cpp:
+    // 313-322): otherwise the shared value (0) enters the RHS.
+    if (noise_std > 0.0) {
+        asg::astro_step_kernel<false, asg::kInputArray, true>
+            <<<grid, block, 0, e->stream>>>(a, e->arrays());
+    } else {
+        a.independent = 0;
+        asg::astro_step_kernel<false, asg::kInputArray, true>
+            <<<grid, block, 0, e->stream>>>(a, e->arrays());
+    }
+    ASG_CUDA(cudaGetLastError());
+    ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
+    e->last_kernels = 1;
+    return ASG_OK;
+}
+
+int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, int32_t substeps,
+                            uint64_t seed, double p, double weight, int64_t first, int64_t count,
+                            int32_t uniform, double Ca_tot, double IP3_0, double tau_IP3,
+                            double delta_IP3) {
+    asg::clear_error();
+    if (s == nullptr || consts == nullptr)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_run_bernoulli: NULL argument");
+    if (count < 0 || first < 0 || substeps < 0)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_run_bernoulli: negative step range");
+    auto* e = reinterpret_cast<AstroEngine*>(s);
+    if (!uniform && e->Ca_tot.get() == nullptr)
+        return asg::fail(ASG_ERR_STATE, "asg_astro_run_bernoulli: no per-cell parameters");
+    if (e->n == 0 || count == 0) {
+        e->last_ms = 0.0;
+        e->last_kernels = 0;
+        return ASG_OK;
+    }
+    asg::StepArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n = e->n;
+    a.k = asg::make_astro_k(consts, h_step, substeps);
+    a.u = asg::UniformParams{Ca_tot, IP3_0, tau_IP3, delta_IP3};
+    a.seed = seed;
+    a.p = p;
+    a.weight = weight;
+    a.step_base = e->step_base.as<std::int64_t>();
+    const int block = 128;
+    const int grid = e->grid_for(std::max<std::int64_t>(1, e->n / 2), block);
+
+    // Steps run as captured chunks of up to 64 launches: kernel j of a chunk
+    // reads step = *step_base + j, and a one-thread node advances the base.
+    const int chunk = static_cast<int>(std::min<std::int64_t>(64, count));
+    auto launch_step = [&](int j) {
+        asg::StepArgs aj = a;
+        aj.step_offset = j;
+        if (uniform) {
+            asg::astro_step_kernel<true, asg::kInputBernoulli, false>
+                <<<grid, block, 0, e->stream>>>(aj, e->arrays());
+        } else {
+            asg::astro_step_kernel<false, asg::kInputBernoulli, false>
+                <<<grid, block, 0, e->stream>>>(aj, e->arrays());
+        }
+    };
+    const bool same = e->graph != nullptr && e->graph_steps == chunk &&
+                      e->graph_uniform == (uniform != 0) &&
+                      std::memcmp(&e->graph_args, &a, sizeof a) == 0;
+    if (!same) {
+        if (e->graph) cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+        cudaGraph_t g = nullptr;
+        ASG_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        for (int j = 0; j < chunk; ++j) launch_step(j);
+        asg::advance_counter_kernel<<<1, 1, 0, e->stream>>>(e->step_base.as<std::int64_t>(), chunk);
+        ASG_CUDA(cudaStreamEndCapture(e->stream, &g));
+        const cudaError_t ce = cudaGraphInstantiate(&e->graph, g, 0);
+        cudaGraphDestroy(g);
+        ASG_CUDA(ce);
+        e->graph_steps = chunk;
+        e->graph_args = a;
+        e->graph_uniform = uniform != 0;
+    }
+    std::int64_t base = first;
+    ASG_CUDA(cudaMemcpyAsync(e->step_base.get(), &base, sizeof base, cudaMemcpyHostToDevice, e->stream));
+    ASG_CUDA(cudaStreamSynchronize(e->stream));
+    ASG_CUDA(cudaEventRecord(e->ev0, e->stream));
+    std::int64_t done = 0;
+    std::int64_t kernels = 0;
+    while (count - done >= chunk) {
+        ASG_CUDA(cudaGraphLaunch(e->graph, e->stream));
+        done += chunk;
+        kernels += chunk + 1;
+    }
+    if (done < count) {
+        // Remainder: plain launches with the base already advanced.
+        for (int j = 0; done + j < count; ++j) launch_step(j);
+        ASG_CUDA(cudaGetLastError());
+        kernels += count - done;
+    }
+    ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
+    ASG_CUDA(cudaEventSynchronize(e->ev1));
+    float ms = 0.0f;
+    ASG_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    e->last_ms = ms;
+    e->last_kernels = kernels;
+    return ASG_OK;
+}
+
+int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels) {
+    asg::clear_error();
+    if (s == nullptr) return asg::fail(ASG_ERR_ARG, "asg_astro_last_timing: NULL handle");
+    auto* e = reinterpret_cast<AstroEngine*>(s);
+    if (device_ms) *device_ms = e->last_ms;
+    if (kernels) *kernels = e->last_kernels;
+    return ASG_OK;
+}
+
+}  // extern "C"

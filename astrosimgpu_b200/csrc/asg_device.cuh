@@ -1,0 +1,221 @@
+// Device-side building blocks shared by every kernel of the engine:
+//   - the counter-based RNG of the model (splitmix64 finaliser over
+//     seed + stream*phi + counter*c, reference rng.hpp:26-50 and the
+//     CounterRng methods rng.hpp:64-124),
+//   - the Li-Rinzel astrocyte right-hand side and its RK4 advance
+//     (reference astrocyte_kernel.hpp:47-103),
+//   - the AdEx right-hand side (reference neuron.cpp:85-99).
+//
+// Bitwise parity with the host build is a design requirement, so every
+// floating-point expression below evaluates the same IEEE operations in the
+// same order as the reference's C++ (left to right, no contraction).  The
+// translation units that include this header are compiled with
+// -fmad=false so nvcc cannot fuse a multiply and an add.  Products of
+// constants that the reference evaluates at run time (for example
+// ratio_ER_cyt * rate_IP3R) are formed once on the host with the same
+// rounding and passed in, which changes no bit of any result.
+#pragma once
+
+#include <cstdint>
+
+namespace asg {
+
+// ------------------------------------------------------------------ RNG
+
+// Golden-ratio increment and the two splitmix64 multipliers (Steele, Lea &
+// Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014).
+constexpr std::uint64_t kPhi = 0x9E3779B97F4A7C15ULL;
+constexpr std::uint64_t kMixA = 0xBF58476D1CE4E5B9ULL;
+constexpr std::uint64_t kMixB = 0x94D049BB133111EBULL;
+
+// Seed salts of the model's independent streams (reference: noise of the
+// astrocytes astrocyte.cpp:318, Poisson drive of neurons neuron.cpp:230,
+// independent neuron noise neuron.cpp:243, shared neuron noise
+// neuron.cpp:204/208, astrocyte Poisson drive network.cpp:461, builder
+// stream network.cpp:57).
+constexpr std::uint64_t kSaltAstroNoise = 0x9E3779B97F4A7C15ULL;
+constexpr std::uint64_t kSaltNeuronPoisson = 0x2545F4914F6CDD1DULL;
+constexpr std::uint64_t kSaltNeuronNoise = 0x9E3779B185EBCA87ULL;
+constexpr std::uint64_t kSaltSharedExc = 0xD1B54A32D192ED03ULL;
+constexpr std::uint64_t kSaltSharedInh = 0xA24BAED4963EE407ULL;
+constexpr std::uint64_t kSaltAstroPoisson = 0xC2B2AE3D27D4EB4FULL;
+// Stream strides: step*1000003+cell (Poisson, astro noise), idx*1000033+cell
+// (neuron noise).
+constexpr std::uint64_t kStreamStride = 1000003ULL;
+constexpr std::uint64_t kNoiseStride = 1000033ULL;
+
+__host__ __device__ __forceinline__ std::uint64_t mix64(std::uint64_t seed, std::uint64_t stream,
+                                                        std::uint64_t counter) {
+    std::uint64_t z = seed + stream * kPhi + counter * kMixA;
+    z = (z ^ (z >> 30)) * kMixA;
+    z = (z ^ (z >> 27)) * kMixB;
+    return z ^ (z >> 31);
+}
+
+// 53 random bits scaled into [0, 1).
+__host__ __device__ __forceinline__ double unit53(std::uint64_t bits) {
+    return static_cast<double>(bits >> 11) * (1.0 / 9007199254740992.0);
+}
+
+__host__ __device__ __forceinline__ double uniform_at(std::uint64_t seed, std::uint64_t stream,
+                                                      std::uint64_t counter) {
+    return unit53(mix64(seed, stream, counter));
+}
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+// Box-Muller cosine branch over counters 0 and 1 with u1 clamped at 1e-300
+// (the free-function form, reference rng.hpp:42-50).
+__device__ __forceinline__ double normal_clamped(std::uint64_t seed, std::uint64_t stream) {
+    double u1 = uniform_at(seed, stream, 0);
+    if (u1 <= 1e-300) u1 = 1e-300;
+    const double u2 = uniform_at(seed, stream, 1);
+    return sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
+}
+
+// Sequential draws of one (seed, stream), the CounterRng object form.
+struct Draws {
+    std::uint64_t seed, stream, counter;
+    __device__ __forceinline__ Draws(std::uint64_t s, std::uint64_t st)
+        : seed(s), stream(st), counter(0) {}
+    __device__ __forceinline__ double uniform() { return uniform_at(seed, stream, counter++); }
+    // First variate of a fresh object: Box-Muller cosine branch, u1 redrawn
+    // while <= 1e-300 (rng.hpp:74-89).  The sine spare is never consumed on
+    // the step path (each object serves one draw), so it is not formed.
+    __device__ __forceinline__ double normal_first() {
+        double u1;
+        do {
+            u1 = uniform();
+        } while (u1 <= 1e-300);
+        const double u2 = uniform();
+        return sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
+    }
+    // Knuth's product method for lambda <= 30 with exp(-lambda) supplied by
+    // the caller (a per-population constant); normal approximation above.
+    __device__ __forceinline__ int poisson(double lambda, double limit) {
+        if (lambda <= 0.0) return 0;
+        if (lambda > 30.0) {
+            const double v = lambda + sqrt(lambda) * normal_first();
+            return v < 0.0 ? 0 : static_cast<int>(v + 0.5);
+        }
+        double product = uniform();
+        int count = 0;
+        while (product > limit) {
+            ++count;
+            product *= uniform();
+        }
+        return count;
+    }
+};
+
+// ------------------------------------------------------ Li-Rinzel astrocyte
+
+// Population constants, with the run-time constant products of the
+// reference's right-hand side pre-formed (same rounding).
+struct AstroK {
+    double Kd_IP3_1, Kd_IP3_2, Kd_act, ratio_ER_cyt;
+    double chan;    // ratio_ER_cyt * rate_IP3R
+    double serca;   // rate_SERCA
+    double km2;     // Km_SERCA * Km_SERCA
+    double leak;    // ratio_ER_cyt * rate_L
+    double ah;      // k_IP3R * Kd_inh
+    double k_IP3R;
+    double half_h;  // 0.5 * h_step
+    double h;       // h_step
+    double h6;      // h_step / 6.0
+    int substeps;
+};
+
+struct AstroRates {
+    double Ca, IP3, h;
+};
+
+// d/dt of (Ca, IP3, h) for one cell.
+__device__ __forceinline__ AstroRates li_rinzel(const AstroK& k, double ca_tot, double ip3_0,
+                                                double tau, double ca, double ip3, double hh,
+                                                double noise) {
+    const double er = (ca_tot - ca) / k.ratio_ER_cyt;  // ER calcium
+    const double ip3_k1 = ip3 + k.Kd_IP3_1;
+    const double m = ip3 / ip3_k1;                      // IP3 activation
+    const double n = ca / (ca + k.Kd_act);              // Ca activation
+    const double m3 = m * m * m;
+    const double n3 = n * n * n;
+    const double h3 = hh * hh * hh;
+    const double gradient = er - ca;
+    const double release = k.chan * m3 * n3 * h3 * gradient;
+    const double ca2 = ca * ca;
+    const double uptake = k.serca * ca * ca / (k.km2 + ca2);
+    const double leak = k.leak * gradient;
+    const double open_rate = k.ah * ip3_k1 / (ip3 + k.Kd_IP3_2);
+    const double close_rate = k.k_IP3R * ca;
+    AstroRates r;
+    r.Ca = release - uptake + leak + noise;
+    r.IP3 = (ip3_0 - ip3) / tau;
+    r.h = open_rate * (1.0 - hh) - close_rate * hh;
+    return r;
+}
+
+// Input jump, then `substeps` classical RK4 steps with the physical clamps.
+__device__ __forceinline__ void astro_rk4(const AstroK& k, double ca_tot, double ip3_0, double tau,
+                                          double delta, double input, double noise, double& ca,
+                                          double& ip3, double& hh) {
+    if (input != 0.0) ip3 += delta * input;
+    for (int s = 0; s < k.substeps; ++s) {
+        const AstroRates a = li_rinzel(k, ca_tot, ip3_0, tau, ca, ip3, hh, noise);
+        const AstroRates b = li_rinzel(k, ca_tot, ip3_0, tau, ca + k.half_h * a.Ca,
+                                       ip3 + k.half_h * a.IP3, hh + k.half_h * a.h, noise);
+        const AstroRates c = li_rinzel(k, ca_tot, ip3_0, tau, ca + k.half_h * b.Ca,
+                                       ip3 + k.half_h * b.IP3, hh + k.half_h * b.h, noise);
+        const AstroRates d = li_rinzel(k, ca_tot, ip3_0, tau, ca + k.h * c.Ca, ip3 + k.h * c.IP3,
+                                       hh + k.h * c.h, noise);
+        ca += k.h6 * (a.Ca + 2.0 * b.Ca + 2.0 * c.Ca + d.Ca);
+        ip3 += k.h6 * (a.IP3 + 2.0 * b.IP3 + 2.0 * c.IP3 + d.IP3);
+        hh += k.h6 * (a.h + 2.0 * b.h + 2.0 * c.h + d.h);
+        ca = ca < 0.0 ? 0.0 : (ca > ca_tot ? ca_tot : ca);
+        hh = hh < 0.0 ? 0.0 : (hh > 1.0 ? 1.0 : hh);
+        ip3 = ip3 < 0.0 ? 0.0 : ip3;
+    }
+}
+
+// ---------------------------------------------------------------- AdEx
+
+// Population constants of one neuron population.
+struct NeuronK {
+    double C_m, g_L, E_L, V_th, Delta_T, a, tau_w, V_peak, E_ex, E_in, I_e;
+    double neg_g_L;      // -g_L
+    double gl_dt;        // g_L * Delta_T
+    double psc_ex, psc_in;           // e / tau_syn (neuron.cpp:157-158)
+    double decay_ex, decay_in;       // exp(-h / tau_syn), host libm
+    int ref_steps;                   // (int)(t_ref / h + 0.5)
+    double poiss_rate, poiss_weight, lambda, knuth_limit;  // lambda = rate*dt*1e-3
+    double noise_std;
+    int independent_noise;
+    int steps_per_noise;
+};
+
+struct AdexRates {
+    double V, w;
+};
+
+// AdEx membrane and adaptation rates.  The spike current is skipped when
+// `with_spike` is false: the refractory branch of the reference evaluates it
+// but only uses dw, which does not depend on it.
+template <bool with_spike>
+__device__ __forceinline__ AdexRates adex(const NeuronK& p, double V, double w, double g_ex,
+                                          double g_in, double I_ext) {
+    const double v = (p.V_peak < V) ? p.V_peak : V;  // std::min(V, V_peak)
+    const double rel = v - p.E_L;
+    AdexRates r;
+    if (with_spike) {
+        const double spike = p.gl_dt * exp((v - p.V_th) / p.Delta_T);
+        const double syn_ex = g_ex * (v - p.E_ex);
+        const double syn_in = g_in * (v - p.E_in);
+        r.V = (p.neg_g_L * rel + spike - syn_ex - syn_in - w + p.I_e + I_ext) / p.C_m;
+    } else {
+        r.V = 0.0;
+    }
+    r.w = (p.a * rel - w) / p.tau_w;
+    return r;
+}
+
+}  // namespace asg

@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 per-timestep engine.
+
+Headline workload (one JSON line on rank 0): the astrocyte kernel-scaling
+case at N = 1e7 independent Li-Rinzel cells (use_case astrocyte parameters,
+IP3 input events Bernoulli(0.01) of weight 0.2 per 0.1 ms step, FP64,
+noise off).  One "step" is one timestep of all N cells.
+
+- value: cell-updates/s with the state resident in HBM, input generated on
+  the device from the counter RNG; device time from CUDA events on the
+  engine's stream, max over ranks.
+- e2e: the same metric through the drop-in C ABI of the reference's CUDA
+  astrocyte backend (asg_astro_push_input / asg_astro_update /
+  asg_astro_pull_calcium), i.e. per step an 8N-byte host->device input copy
+  and an 8N-byte device->host calcium copy from pinned host memory, exactly
+  the movement pattern of the reference's published GPU numbers.
+- roofline: algorithmic HBM bytes of the step kernel (Ca, IP3, h read and
+  written: 48 B per cell-step) / measured launch time, against the measured
+  HBM copy bandwidth.
+- cpu_baseline: the reference's own astro_advance (built from its sources,
+  oracle/_ref) over a bounded sample on the host cores with OpenMP.
+- reference_cuda_kernel: the reference's astro_update_kernel built for
+  sm_100a, timed on the same GPU (the GPU bar to beat).
+- network / batched / serving sub-objects: see --help.
+
+Multi-GPU: the astrocyte cells are independent, so N GPUs each run their
+own N-cell instance (weak scaling, no collective); rank 0 reports the sum.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "neuron-updates/s & HBM GB/s vs roofline; batched/served vs plain; p50/p99 lat"
+BYTES_PER_CELL_STEP = 48  # Ca, IP3, h: read + write, FP64
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if os.environ.get("ASG_BENCH_GLOO") is None else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def pinned(n):
+    """Pinned host float64 buffer as a numpy array (torch allocates it)."""
+    import torch
+    t = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    import numpy as np
+    arr = t.numpy()
+    return t, arr
+
+
+def bench_astro_scaling(args, rank, world, pg):
+    import numpy as np
+    import torch
+
+    from astrosimgpu_b200.astro import AstroBackend, ScalingWorkload
+
+    n = args.cells
+    w = ScalingWorkload(n, seed=1 + rank)
+    Ca, IP3, h = w.initial_state()
+    eng = AstroBackend(Ca, IP3, h)
+    # warm-up (untimed)
+    step = 0
+    for _ in range(args.warmup):
+        eng.run_bernoulli(w, step, 1)
+        step += 1
+    torch.cuda.synchronize()
+    barrier(pg)
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        dev_ms, kernels = eng.run_bernoulli(w, step, args.steps)
+        torch.cuda.synchronize()
+    barrier(pg)
+    step += args.steps
+    dev_ms = max_over_ranks(pg, dev_ms)
+    per_launch_us = dev_ms * 1e3 / args.steps
+    value = n * world * args.steps / (dev_ms * 1e-3)
+
+    # e2e through the drop-in ABI: H2D input + update + D2H Ca per step.
+    ein_t, ein = pinned(n)
+    eca_t, eca = pinned(n)
+    rng_inputs = []
+    cells = np.arange(n, dtype=np.uint64)
+    from astrosimgpu_b200.astro import uniform_np
+    for k in range(2):
+        u = uniform_np(w.seed, cells, 1000 + 10_000 + k)
+        rng_inputs.append(np.where(u < w.p, w.weight, 0.0))
+    e2e_steps = max(3, min(args.steps, 20))
+    for k in range(2):  # warm-up of the copy path
+        ein[:] = rng_inputs[k % 2]
+        eng.push_input(ein)
+        eng.update(w.consts, w.h_step, w.substeps)
+        eca[:] = eng.pull_calcium()
+    torch.cuda.synchronize()
+    barrier(pg)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev0.record()
+    lib = eng  # noqa: F841
+    from astrosimgpu_b200 import _lib
+    L = _lib.load()
+    for k in range(e2e_steps):
+        ein[:] = rng_inputs[k % 2]
+        _lib.check(L.asg_astro_push_input(eng._h, _lib.dptr(ein)), "push")
+        _lib.check(L.asg_astro_update(eng._h, _lib.dptr(w.consts), w.h_step, w.substeps, 0.0, 1,
+                                      0.0, 0, 0), "update")
+        _lib.check(L.asg_astro_pull_calcium(eng._h, _lib.dptr(eca)), "pull")
+    ev1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier(pg)
+    wall = max_over_ranks(pg, wall)
+    e2e_value = n * world * e2e_steps / wall
+    del ein_t, eca_t
+
+    peak, peak_kind = load_peaks()
+    achieved = BYTES_PER_CELL_STEP * n / (per_launch_us * 1e-6) / 1e9
+    out = {
+        "value": value, "ms_per_step": dev_ms / args.steps, "kernels": kernels,
+        "per_launch_us": per_launch_us,
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s",
+                "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                "steps": e2e_steps, "path": "asg_astro_push_input+update+pull_calcium"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": peak_kind,
+                     "bytes_per_launch": BYTES_PER_CELL_STEP * n,
+                     "kernel": "astro_step_kernel<uniform,bernoulli>"},
+        "clocks": clk.summary(),
+    }
+    return out, (w, Ca, IP3, h)
+
+
+def reference_cuda_kernel(w, Ca, IP3, h, steps):
+    """The reference's astro_update_kernel (sm_100a build) on the same GPU."""
+    import numpy as np
+
+    from oracle import ref
+    lib = ref.refcu()
+    n = len(Ca)
+    Ca_tot = np.full(n, w.Ca_tot)
+    IP3_0 = np.full(n, w.IP3_0)
+    tau = np.full(n, w.tau_IP3)
+    delta = np.full(n, w.delta_IP3)
+    arrs = [np.ascontiguousarray(a) for a in (Ca, IP3, h, Ca_tot, IP3_0, tau, delta)]
+    s = lib.refcu_create(n, *[ref._dp(a) for a in arrs])
+    lib.refcu_time_updates(s, ref._dp(w.consts), w.h_step, w.substeps, 3)
+    ms = lib.refcu_time_updates(s, ref._dp(w.consts), w.h_step, w.substeps, steps)
+    o = [np.empty(n) for _ in range(3)]
+    lib.refcu_destroy(s, *[ref._dp(a) for a in o])
+    us = ms * 1e3 / steps
+    return {"us_per_step": us, "cell_updates_per_s": n / (us * 1e-6), "steps": steps,
+            "note": "reference astro_update_kernel, block 128, built -arch sm_100a, "
+                    "resident state, no copies"}
+
+
+def cpu_baseline(w, budget_s=12.0):
+    """Reference astro_advance on the host cores (OpenMP), bounded sample."""
+    import numpy as np
+
+    from oracle import ref
+    lib = ref.ref()
+    threads = os.cpu_count() or 1
+    n = w.n
+    Ca, IP3, h = [a.copy() for a in w.initial_state()]
+    ref.ref_astro_scaling(w, Ca, IP3, h, 0, 1, threads=threads)  # warm
+    steps, secs = 0, 0.0
+    while secs < budget_s and steps < 1000:
+        secs += ref.ref_astro_scaling(w, Ca, IP3, h, 1 + steps, 1, threads=threads)
+        steps += 1
+    del np
+    return {"value": n * steps / secs, "unit": "cell-updates/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{steps} steps x {n} cells of the same workload through the reference's "
+                      f"astro_advance (OpenMP, {threads} threads, oracle/_ref)",
+            "omp_max_threads": int(lib.ref_omp_max_threads())}
+
+
+def run_reference_arm(args, rank, world, pg):
+    """--impl reference: the reference's CPU implementation on the host cores."""
+    if rank != 0:
+        return 0
+    from astrosimgpu_b200.astro import ScalingWorkload
+
+    from oracle import ref
+    threads = os.cpu_count() or 1
+    w = ScalingWorkload(args.cells)
+    Ca, IP3, h = [a.copy() for a in w.initial_state()]
+    step = 0
+    for _ in range(args.warmup):
+        ref.ref_astro_scaling(w, Ca, IP3, h, step, 1, threads=threads)
+        step += 1
+    secs = ref.ref_astro_scaling(w, Ca, IP3, h, step, args.steps, threads=threads)
+    value = args.cells * args.steps / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"astrocyte kernel scaling, N={args.cells}, 1 step = 1 timestep "
+                               "(0.1 ms) of all cells, Bernoulli(0.01) IP3 input w=0.2",
+                   "cells": args.cells},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{args.steps} full steps of {args.cells} cells through the "
+                                   "reference's astro_advance (OpenMP), oracle/_ref"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cells", type=int, default=10_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the reference CUDA kernel and sub-benchmarks")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    if args.impl == "reference":
+        rc = run_reference_arm(args, rank, world, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return rc
+
+    import torch
+    torch.cuda.set_device(local)
+    res, (w, Ca, IP3, h) = bench_astro_scaling(args, rank, world, pg)
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        try:
+            extras["reference_cuda_kernel"] = reference_cuda_kernel(w, Ca, IP3, h,
+                                                                    min(args.steps, 50))
+        except Exception as e:  # noqa: BLE001
+            extras["reference_cuda_kernel"] = {"unavailable": str(e)[:200]}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": res["value"], "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"astrocyte kernel scaling, N={args.cells} per GPU, 1 step = "
+                                   "1 timestep (0.1 ms) of all cells, Bernoulli(0.01) IP3 input "
+                                   "w=0.2, use_case astrocyte parameters, noise off",
+                       "cells_per_gpu": args.cells, "parallelism": f"replicas x{world}",
+                       "l2": "working set 24 B/cell = 240 MB > 126 MB L2 (no flush needed)"},
+            "e2e": res["e2e"], "gpu_launches": res["kernels"], "roofline": res["roofline"],
+            "clocks": res["clocks"], "per_launch_us": res["per_launch_us"],
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
