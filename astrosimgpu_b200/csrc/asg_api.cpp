@@ -1,0 +1,314 @@
+// C ABI of the network engine: the single-network handle (asg_*) and the
+// batched sweep (asg_batch_*).  Both are thin shells over asg::Engine; a
+// plain network is an engine holding one instance.
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "asg_engine.hpp"
+
+namespace asg {
+
+EngineConfig config_from(const asg_engine_opts* o) {
+    EngineConfig c;
+    if (o != nullptr) {
+        c.device = o->device;
+        if (o->chunk_steps > 0) c.chunk_steps = o->chunk_steps;
+        const int b = o->block_neuron > 0 ? o->block_neuron : 0;
+        if (b > 0) c.block = b;
+        if (o->use_graphs != 0) c.use_graphs = o->use_graphs;
+        c.sic_mode = o->sic_mode;
+        c.mem_budget = o->mem_budget;
+    }
+    return c;
+}
+
+namespace {
+
+int fetch_spikes_from(Instance* I, int64_t* steps, uint32_t* sources, int64_t cap,
+                      int64_t* count) {
+    const int64_t n = static_cast<int64_t>(I->spikes.size());
+    if (count) *count = n;
+    if (steps == nullptr && sources == nullptr) return ASG_OK;  // size query
+    if (n > cap) return fail(ASG_ERR_OVERFLOW, "%lld spikes pending, buffer holds %lld",
+                             static_cast<long long>(n), static_cast<long long>(cap));
+    for (int64_t i = 0; i < n; ++i) {
+        if (steps) steps[i] = I->spikes[i].step;
+        if (sources) sources[i] = I->spikes[i].source;
+    }
+    I->spikes.clear();
+    return ASG_OK;
+}
+
+int fetch_record_from(Instance* I, int64_t* astro_steps, double* Ca, double* IP3,
+                      int64_t astro_cap, int64_t* astro_rows, int64_t* neuron_steps, double* V,
+                      double* Isic, int64_t neuron_cap, int64_t* neuron_rows) {
+    const int64_t na = static_cast<int64_t>(I->astro_rec_steps.size());
+    const int64_t nn = static_cast<int64_t>(I->neuron_rec_steps.size());
+    if (astro_rows) *astro_rows = na;
+    if (neuron_rows) *neuron_rows = nn;
+    const bool want_a = astro_steps || Ca || IP3;
+    const bool want_n = neuron_steps || V || Isic;
+    if (want_a && na > astro_cap)
+        return fail(ASG_ERR_OVERFLOW, "%lld astrocyte rows pending, buffer holds %lld",
+                    static_cast<long long>(na), static_cast<long long>(astro_cap));
+    if (want_n && nn > neuron_cap)
+        return fail(ASG_ERR_OVERFLOW, "%lld neuron rows pending, buffer holds %lld",
+                    static_cast<long long>(nn), static_cast<long long>(neuron_cap));
+    if (want_a) {
+        if (astro_steps) std::copy(I->astro_rec_steps.begin(), I->astro_rec_steps.end(), astro_steps);
+        if (Ca) std::copy(I->rec_Ca.begin(), I->rec_Ca.end(), Ca);
+        if (IP3) std::copy(I->rec_IP3.begin(), I->rec_IP3.end(), IP3);
+        I->astro_rec_steps.clear();
+        I->rec_Ca.clear();
+        I->rec_IP3.clear();
+    }
+    if (want_n) {
+        if (neuron_steps) std::copy(I->neuron_rec_steps.begin(), I->neuron_rec_steps.end(), neuron_steps);
+        if (V) std::copy(I->rec_V.begin(), I->rec_V.end(), V);
+        if (Isic) std::copy(I->rec_Isic.begin(), I->rec_Isic.end(), Isic);
+        I->neuron_rec_steps.clear();
+        I->rec_V.clear();
+        I->rec_Isic.clear();
+    }
+    return ASG_OK;
+}
+
+}  // namespace
+
+struct NetworkHandle {
+    std::unique_ptr<Engine> eng;
+    int id = -1;
+};
+
+struct BatchHandle {
+    std::unique_ptr<Engine> eng;
+    std::vector<int> ids;
+};
+
+}  // namespace asg
+
+using asg::BatchHandle;
+using asg::Engine;
+using asg::NetworkHandle;
+
+extern "C" {
+
+int asg_create(const asg_network_desc* desc, const asg_record_opts* rec,
+               const asg_engine_opts* opts, asg_network** out) {
+    asg::clear_error();
+    if (desc == nullptr || out == nullptr) return asg::fail(ASG_ERR_ARG, "asg_create: NULL argument");
+    *out = nullptr;
+    auto h = std::make_unique<NetworkHandle>();
+    h->eng = std::make_unique<Engine>(asg::config_from(opts));
+    ASG_TRY(h->eng->init());
+    ASG_TRY(h->eng->add(*desc, rec, 0, INT64_MAX, true, &h->id));
+    *out = reinterpret_cast<asg_network*>(h.release());
+    return ASG_OK;
+}
+
+int asg_step(asg_network* net, int64_t n_steps) {
+    asg::clear_error();
+    if (net == nullptr) return asg::fail(ASG_ERR_ARG, "asg_step: NULL handle");
+    return reinterpret_cast<NetworkHandle*>(net)->eng->run(n_steps);
+}
+
+int asg_current_step(asg_network* net, int64_t* step) {
+    asg::clear_error();
+    if (net == nullptr || step == nullptr) return asg::fail(ASG_ERR_ARG, "asg_current_step: NULL");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    *step = h->eng->find(h->id)->step;
+    return ASG_OK;
+}
+
+int asg_fetch_spikes(asg_network* net, int64_t* steps, uint32_t* sources, int64_t cap,
+                     int64_t* count) {
+    asg::clear_error();
+    if (net == nullptr) return asg::fail(ASG_ERR_ARG, "asg_fetch_spikes: NULL handle");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    return asg::fetch_spikes_from(h->eng->find(h->id), steps, sources, cap, count);
+}
+
+int asg_fetch_record(asg_network* net, int64_t* astro_steps, double* Ca, double* IP3,
+                     int64_t astro_cap_rows, int64_t* astro_rows, int64_t* neuron_steps,
+                     double* V, double* I_sic, int64_t neuron_cap_rows, int64_t* neuron_rows) {
+    asg::clear_error();
+    if (net == nullptr) return asg::fail(ASG_ERR_ARG, "asg_fetch_record: NULL handle");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    return asg::fetch_record_from(h->eng->find(h->id), astro_steps, Ca, IP3, astro_cap_rows,
+                                  astro_rows, neuron_steps, V, I_sic, neuron_cap_rows,
+                                  neuron_rows);
+}
+
+int asg_pull_state(asg_network* net, asg_state* out) {
+    asg::clear_error();
+    if (net == nullptr || out == nullptr) return asg::fail(ASG_ERR_ARG, "asg_pull_state: NULL");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    return h->eng->pull_state(h->id, out);
+}
+
+int asg_pull_stp(asg_network* net, double* x, double* u, double* t_last) {
+    asg::clear_error();
+    if (net == nullptr) return asg::fail(ASG_ERR_ARG, "asg_pull_stp: NULL handle");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    return h->eng->pull_stp(h->id, x, u, t_last);
+}
+
+int asg_counters(asg_network* net, int64_t* spike_edges, int64_t* sic_edges, int64_t* spikes) {
+    asg::clear_error();
+    if (net == nullptr) return asg::fail(ASG_ERR_ARG, "asg_counters: NULL handle");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    const asg::Instance* I = h->eng->find(h->id);
+    if (spike_edges) *spike_edges = I->spike_edges;
+    if (sic_edges) *sic_edges = I->sic_edges;
+    if (spikes) *spikes = I->n_spikes;
+    return ASG_OK;
+}
+
+int asg_last_timing(asg_network* net, double* device_ms, int64_t* kernels) {
+    asg::clear_error();
+    if (net == nullptr) return asg::fail(ASG_ERR_ARG, "asg_last_timing: NULL handle");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    if (device_ms) *device_ms = h->eng->last_ms;
+    if (kernels) *kernels = h->eng->last_kernels;
+    return ASG_OK;
+}
+
+int asg_checkpoint_size(asg_network* net, uint64_t* bytes) {
+    asg::clear_error();
+    if (net == nullptr || bytes == nullptr) return asg::fail(ASG_ERR_ARG, "asg_checkpoint_size: NULL");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    *bytes = h->eng->find(h->id)->arena_bytes + sizeof(int64_t);
+    return ASG_OK;
+}
+
+int asg_checkpoint(asg_network* net, void* host_buf, uint64_t bytes) {
+    asg::clear_error();
+    if (net == nullptr || host_buf == nullptr) return asg::fail(ASG_ERR_ARG, "asg_checkpoint: NULL");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    asg::Instance* I = h->eng->find(h->id);
+    if (bytes < I->arena_bytes + sizeof(int64_t))
+        return asg::fail(ASG_ERR_OVERFLOW, "checkpoint needs %zu bytes", I->arena_bytes + 8);
+    ASG_CUDA(cudaStreamSynchronize(h->eng->stream));
+    std::memcpy(host_buf, &I->step, sizeof(int64_t));
+    ASG_CUDA(cudaMemcpy(static_cast<char*>(host_buf) + 8, I->arena.get(), I->arena_bytes,
+                        cudaMemcpyDeviceToHost));
+    return ASG_OK;
+}
+
+int asg_restore(asg_network* net, const void* host_buf, uint64_t bytes) {
+    asg::clear_error();
+    if (net == nullptr || host_buf == nullptr) return asg::fail(ASG_ERR_ARG, "asg_restore: NULL");
+    auto* h = reinterpret_cast<NetworkHandle*>(net);
+    asg::Instance* I = h->eng->find(h->id);
+    if (bytes != I->arena_bytes + sizeof(int64_t))
+        return asg::fail(ASG_ERR_ARG, "checkpoint size %llu does not match this network (%zu)",
+                         static_cast<unsigned long long>(bytes), I->arena_bytes + 8);
+    ASG_CUDA(cudaStreamSynchronize(h->eng->stream));
+    std::memcpy(&I->step, host_buf, sizeof(int64_t));
+    ASG_CUDA(cudaMemcpy(I->arena.get(), static_cast<const char*>(host_buf) + 8, I->arena_bytes,
+                        cudaMemcpyHostToDevice));
+    I->spikes.clear();
+    return ASG_OK;
+}
+
+int asg_destroy(asg_network* net) {
+    asg::clear_error();
+    delete reinterpret_cast<NetworkHandle*>(net);
+    return ASG_OK;
+}
+
+// ------------------------------------------------------------------ batch
+
+int asg_batch_create(int32_t n, const asg_network_desc* const* descs, const asg_record_opts* rec,
+                     const asg_engine_opts* opts, asg_batch** out) {
+    asg::clear_error();
+    if (out == nullptr || (n > 0 && descs == nullptr) || n < 0)
+        return asg::fail(ASG_ERR_ARG, "asg_batch_create: bad arguments");
+    *out = nullptr;
+    auto h = std::make_unique<BatchHandle>();
+    h->eng = std::make_unique<Engine>(asg::config_from(opts));
+    ASG_TRY(h->eng->init());
+    for (int32_t i = 0; i < n; ++i) {
+        if (descs[i] == nullptr) return asg::fail(ASG_ERR_ARG, "asg_batch_create: descs[%d] NULL", i);
+        int id = -1;
+        const int st = h->eng->add(*descs[i], rec, 0, INT64_MAX, true, &id);
+        if (st != ASG_OK) return st;
+        h->ids.push_back(id);
+    }
+    *out = reinterpret_cast<asg_batch*>(h.release());
+    return ASG_OK;
+}
+
+static asg::Instance* batch_inst(asg_batch* b, int32_t inst) {
+    auto* h = reinterpret_cast<BatchHandle*>(b);
+    if (inst < 0 || inst >= static_cast<int32_t>(h->ids.size())) return nullptr;
+    return h->eng->find(h->ids[inst]);
+}
+
+int asg_batch_step(asg_batch* b, int64_t n_steps) {
+    asg::clear_error();
+    if (b == nullptr) return asg::fail(ASG_ERR_ARG, "asg_batch_step: NULL handle");
+    return reinterpret_cast<BatchHandle*>(b)->eng->run(n_steps);
+}
+
+int asg_batch_fetch_spikes(asg_batch* b, int32_t inst, int64_t* steps, uint32_t* sources,
+                           int64_t cap, int64_t* count) {
+    asg::clear_error();
+    if (b == nullptr) return asg::fail(ASG_ERR_ARG, "asg_batch_fetch_spikes: NULL handle");
+    asg::Instance* I = batch_inst(b, inst);
+    if (I == nullptr) return asg::fail(ASG_ERR_NOT_FOUND, "no instance %d", inst);
+    return asg::fetch_spikes_from(I, steps, sources, cap, count);
+}
+
+int asg_batch_fetch_record(asg_batch* b, int32_t inst, int64_t* astro_steps, double* Ca,
+                           double* IP3, int64_t astro_cap_rows, int64_t* astro_rows,
+                           int64_t* neuron_steps, double* V, double* I_sic,
+                           int64_t neuron_cap_rows, int64_t* neuron_rows) {
+    asg::clear_error();
+    if (b == nullptr) return asg::fail(ASG_ERR_ARG, "asg_batch_fetch_record: NULL handle");
+    asg::Instance* I = batch_inst(b, inst);
+    if (I == nullptr) return asg::fail(ASG_ERR_NOT_FOUND, "no instance %d", inst);
+    return asg::fetch_record_from(I, astro_steps, Ca, IP3, astro_cap_rows, astro_rows,
+                                  neuron_steps, V, I_sic, neuron_cap_rows, neuron_rows);
+}
+
+int asg_batch_pull_state(asg_batch* b, int32_t inst, asg_state* out) {
+    asg::clear_error();
+    if (b == nullptr || out == nullptr) return asg::fail(ASG_ERR_ARG, "asg_batch_pull_state: NULL");
+    auto* h = reinterpret_cast<BatchHandle*>(b);
+    if (inst < 0 || inst >= static_cast<int32_t>(h->ids.size()))
+        return asg::fail(ASG_ERR_NOT_FOUND, "no instance %d", inst);
+    return h->eng->pull_state(h->ids[inst], out);
+}
+
+int asg_batch_counters(asg_batch* b, int32_t inst, int64_t* spike_edges, int64_t* sic_edges,
+                       int64_t* spikes) {
+    asg::clear_error();
+    if (b == nullptr) return asg::fail(ASG_ERR_ARG, "asg_batch_counters: NULL handle");
+    asg::Instance* I = batch_inst(b, inst);
+    if (I == nullptr) return asg::fail(ASG_ERR_NOT_FOUND, "no instance %d", inst);
+    if (spike_edges) *spike_edges = I->spike_edges;
+    if (sic_edges) *sic_edges = I->sic_edges;
+    if (spikes) *spikes = I->n_spikes;
+    return ASG_OK;
+}
+
+int asg_batch_last_timing(asg_batch* b, double* device_ms, int64_t* kernels) {
+    asg::clear_error();
+    if (b == nullptr) return asg::fail(ASG_ERR_ARG, "asg_batch_last_timing: NULL handle");
+    auto* h = reinterpret_cast<BatchHandle*>(b);
+    if (device_ms) *device_ms = h->eng->last_ms;
+    if (kernels) *kernels = h->eng->last_kernels;
+    return ASG_OK;
+}
+
+int asg_batch_destroy(asg_batch* b) {
+    asg::clear_error();
+    delete reinterpret_cast<BatchHandle*>(b);
+    return ASG_OK;
+}
+
+}  // extern "C"

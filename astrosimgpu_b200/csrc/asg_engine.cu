@@ -1,0 +1,816 @@
+// Host side of the network engine (see asg_engine.hpp / asg_engine.cuh):
+// descriptor validation, table preprocessing, the per-instance device arena,
+// the work table, captured chunks and output collection.
+
+#include "asg_engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace asg {
+
+namespace {
+
+constexpr double kE = 2.7182818284590452353602874713527;
+
+int delay_ok(int d) { return d >= 1; }
+
+// Derived constants of one neuron population (values the reference forms at
+// run time are formed here with the same IEEE operations).
+NeuronK make_neuron_k(const asg_neuron_params& p, const asg_input& in, double dt, double h) {
+    NeuronK k{};
+    k.C_m = p.C_m;
+    k.g_L = p.g_L;
+    k.E_L = p.E_L;
+    k.V_th = p.V_th;
+    k.Delta_T = p.Delta_T;
+    k.a = p.a;
+    k.tau_w = p.tau_w;
+    k.V_peak = p.V_peak;
+    k.E_ex = p.E_ex;
+    k.E_in = p.E_in;
+    k.I_e = p.I_e;
+    k.neg_g_L = -p.g_L;
+    k.gl_dt = p.g_L * p.Delta_T;
+    k.psc_ex = kE / p.tau_syn_ex;
+    k.psc_in = kE / p.tau_syn_in;
+    k.decay_ex = std::exp(-h / p.tau_syn_ex);
+    k.decay_in = std::exp(-h / p.tau_syn_in);
+    k.ref_steps = static_cast<int>(p.t_ref / h + 0.5);
+    k.poiss_rate = in.poiss_rate;
+    k.poiss_weight = in.poiss_weight;
+    k.lambda = in.poiss_rate * dt * 1e-3;
+    k.knuth_limit = std::exp(-k.lambda);
+    k.noise_std = in.gauss_noise_std;
+    k.independent_noise = in.independent_noise != 0;
+    k.steps_per_noise = std::max(1, static_cast<int>(std::llround(in.noise_dt / dt)));
+    return k;
+}
+
+AstroK make_astro_k(const asg_astro_params& a, double h, int substeps) {
+    AstroK k{};
+    k.Kd_IP3_1 = a.Kd_IP3_1;
+    k.Kd_IP3_2 = a.Kd_IP3_2;
+    k.Kd_act = a.Kd_act;
+    k.ratio_ER_cyt = a.ratio_ER_cyt;
+    k.chan = a.ratio_ER_cyt * a.rate_IP3R;
+    k.serca = a.rate_SERCA;
+    k.km2 = a.Km_SERCA * a.Km_SERCA;
+    k.leak = a.ratio_ER_cyt * a.rate_L;
+    k.ah = a.k_IP3R * a.Kd_inh;
+    k.k_IP3R = a.k_IP3R;
+    k.half_h = 0.5 * h;
+    k.h = h;
+    k.h6 = h / 6.0;
+    k.substeps = substeps;
+    return k;
+}
+
+// Transposed in-edge structure of one set (host arrays).
+struct InRingHost {
+    std::vector<std::uint32_t> row, src, wbase, bitpos;
+    std::uint32_t words = 0;
+};
+
+InRingHost make_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std::uint32_t* tg,
+                        std::uint32_t n_targets) {
+    InRingHost r;
+    const std::uint32_t m = rs[n_src];
+    r.row.assign(n_targets + 1, 0);
+    for (std::uint32_t e = 0; e < m; ++e) r.row[tg[e] + 1]++;
+    for (std::uint32_t t = 0; t < n_targets; ++t) r.row[t + 1] += r.row[t];
+    r.wbase.assign(n_targets + 1, 0);
+    for (std::uint32_t t = 0; t < n_targets; ++t) {
+        const std::uint32_t deg = r.row[t + 1] - r.row[t];
+        r.wbase[t + 1] = r.wbase[t] + (deg + 31) / 32;
+    }
+    r.words = r.wbase[n_targets];
+    r.src.assign(m, 0);
+    r.bitpos.assign(m, 0);
+    std::vector<std::uint32_t> fill(r.row.begin(), r.row.end() - 1);
+    // Sources ascending, each row in CSR order: every in-list comes out
+    // sorted by (source, position in the source's row).
+    for (std::uint32_t s = 0; s < n_src; ++s) {
+        for (std::uint32_t e = rs[s]; e < rs[s + 1]; ++e) {
+            const std::uint32_t t = tg[e];
+            const std::uint32_t p = fill[t]++;
+            r.src[p] = s;
+            r.bitpos[e] = r.wbase[t] * 32 + (p - r.row[t]);
+        }
+    }
+    return r;
+}
+
+// Compressed SIC lists in sliced ELL (32 targets per slice).
+struct SicHost {
+    std::vector<std::uint32_t> soff, ent;
+};
+
+SicHost make_sic(std::uint32_t NA, const std::uint32_t* rs, const std::uint32_t* tg,
+                 std::uint32_t N) {
+    // per target: (astro, mult) in ascending astro order
+    std::vector<std::vector<std::uint32_t>> lists(N);
+    for (std::uint32_t a = 0; a < NA; ++a) {
+        for (std::uint32_t e = rs[a]; e < rs[a + 1]; ++e) {
+            auto& l = lists[tg[e]];
+            if (!l.empty() && (l.back() >> 8) == a && (l.back() & 0xFFu) < 255u) {
+                l.back() += 1;
+            } else {
+                l.push_back((a << 8) | 1u);
+            }
+        }
+    }
+    SicHost s;
+    const std::uint32_t slices = (N + 31) / 32;
+    s.soff.assign(slices + 1, 0);
+    for (std::uint32_t sl = 0; sl < slices; ++sl) {
+        std::size_t len = 0;
+        for (std::uint32_t t = sl * 32; t < std::min(N, sl * 32 + 32); ++t)
+            len = std::max(len, lists[t].size());
+        s.soff[sl + 1] = s.soff[sl] + static_cast<std::uint32_t>(len * 32);
+    }
+    s.ent.assign(std::max<std::uint32_t>(s.soff[slices], 1), 0u);
+    for (std::uint32_t t = 0; t < N; ++t) {
+        const std::uint32_t sl = t / 32, lane = t % 32;
+        for (std::size_t q = 0; q < lists[t].size(); ++q)
+            s.ent[s.soff[sl] + q * 32 + lane] = lists[t][q];
+    }
+    return s;
+}
+
+int check_csr(const char* name, const asg_csr& c, std::uint32_t n_src, std::uint32_t n_tgt) {
+    if (c.n_sources != n_src)
+        return fail(ASG_ERR_ARG, "%s: n_sources %u, expected %u", name, c.n_sources, n_src);
+    if (n_src > 0 && (c.row_start == nullptr))
+        return fail(ASG_ERR_ARG, "%s: row_start is NULL", name);
+    if (n_src == 0) return ASG_OK;
+    if (c.row_start[0] != 0) return fail(ASG_ERR_ARG, "%s: row_start[0] != 0", name);
+    for (std::uint32_t s = 0; s < n_src; ++s)
+        if (c.row_start[s + 1] < c.row_start[s])
+            return fail(ASG_ERR_ARG, "%s: row_start decreases at %u", name, s);
+    const std::uint32_t m = c.row_start[n_src];
+    if (m > 0 && c.target == nullptr) return fail(ASG_ERR_ARG, "%s: target is NULL", name);
+    for (std::uint32_t e = 0; e < m; ++e)
+        if (c.target[e] >= n_tgt)
+            return fail(ASG_ERR_ARG, "%s: target[%u] = %u out of range (%u)", name, e,
+                        c.target[e], n_tgt);
+    return ASG_OK;
+}
+
+int check_uniform(const char* name, const asg_csr& c, std::uint32_t n_src, double w, int d,
+                  const asg_stp& stp) {
+    if (n_src == 0) return ASG_OK;
+    const std::uint32_t m = c.row_start[n_src];
+    for (std::uint32_t e = 0; e < m; ++e) {
+        if (c.weight && c.weight[e] != w)
+            return fail(ASG_ERR_UNSUPPORTED,
+                        "%s: per-edge weight %g differs from the set weight %g (the engine "
+                        "takes one weight per set, as the reference builds them)",
+                        name, c.weight[e], w);
+        if (c.delay_steps && c.delay_steps[e] != d)
+            return fail(ASG_ERR_UNSUPPORTED, "%s: per-edge delay %d differs from the set delay %d",
+                        name, c.delay_steps[e], d);
+    }
+    if (stp.enabled && (c.stp_x || c.stp_u || c.stp_t_last)) {
+        for (std::uint32_t s = 0; s < n_src; ++s) {
+            for (std::uint32_t e = c.row_start[s]; e < c.row_start[s + 1]; ++e) {
+                const std::uint32_t f = c.row_start[s];
+                if ((c.stp_x && c.stp_x[e] != c.stp_x[f]) || (c.stp_u && c.stp_u[e] != c.stp_u[f]) ||
+                    (c.stp_t_last && c.stp_t_last[e] != c.stp_t_last[f]))
+                    return fail(ASG_ERR_UNSUPPORTED,
+                                "%s: STP state differs along the row of source %u", name, s);
+            }
+        }
+    }
+    return ASG_OK;
+}
+
+bool all_equal(const double* a, std::uint32_t n) {
+    for (std::uint32_t i = 1; i < n; ++i)
+        if (std::memcmp(&a[i], &a[0], sizeof(double)) != 0) return false;
+    return true;
+}
+
+// Arena layout: a list of (destination pointer, bytes, host source) entries
+// placed at 256-byte boundaries in one allocation.
+struct Seg {
+    void* dst;  // address of the pointer field to set
+    std::size_t bytes;
+    const void* src;  // nullptr: zero-filled
+};
+
+std::size_t align256(std::size_t x) { return (x + 255) & ~static_cast<std::size_t>(255); }
+
+}  // namespace
+
+Instance::~Instance() {
+    for (int p = 0; p < 2; ++p) {
+        if (log_h[p]) cudaFreeHost(log_h[p]);
+        if (rec_h[p]) cudaFreeHost(rec_h[p]);
+    }
+}
+
+Engine::Engine(const EngineConfig& c) : cfg(c) {}
+
+Engine::~Engine() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (int p = 0; p < 2; ++p) {
+        if (h_insts[p]) cudaFreeHost(h_insts[p]);
+        if (h_stats[p]) cudaFreeHost(h_stats[p]);
+        if (ev_chunk[p]) cudaEventDestroy(ev_chunk[p]);
+    }
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_end) cudaEventDestroy(ev_end);
+    insts.clear();
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int Engine::init() {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return fail(ASG_ERR_NO_DEVICE, "no CUDA device visible");
+    if (cfg.device < 0 || cfg.device >= count)
+        return fail(ASG_ERR_ARG, "device %d out of range (%d devices)", cfg.device, count);
+    ASG_CUDA(cudaSetDevice(cfg.device));
+    ASG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg.device));
+    if (cfg.chunk_steps <= 0) cfg.chunk_steps = 32;
+    if (cfg.block <= 0) cfg.block = 128;
+    if (cfg.block > 512 || cfg.block % 32 != 0)
+        return fail(ASG_ERR_ARG, "block size %d must be a multiple of 32 in [32, 512]", cfg.block);
+    if (cfg.mem_budget == 0) {
+        std::size_t fr = 0, tot = 0;
+        ASG_CUDA(cudaMemGetInfo(&fr, &tot));
+        cfg.mem_budget = static_cast<std::uint64_t>(0.9 * static_cast<double>(fr));
+    }
+    ASG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    ASG_CUDA(cudaEventCreate(&ev_start));
+    ASG_CUDA(cudaEventCreate(&ev_end));
+    for (int p = 0; p < 2; ++p) ASG_CUDA(cudaEventCreateWithFlags(&ev_chunk[p], cudaEventDisableTiming));
+    return ASG_OK;
+}
+
+Instance* Engine::find(int id) {
+    for (auto& p : insts)
+        if (p->id == id) return p.get();
+    return nullptr;
+}
+
+int Engine::footprint(const asg_network_desc& d, int chunk_steps, std::uint64_t* bytes) {
+    // Upper estimate from sizes alone (no preprocessing), used for admission.
+    const std::uint64_t N = d.n_exc + d.n_inh, NA = d.n_astro;
+    const int md = std::max({1, d.d_e_steps, d.d_i_steps, d.d_a2n_steps});
+    const std::uint64_t slots = md + 1;
+    auto edges = [](const asg_csr& c) -> std::uint64_t {
+        return c.n_sources && c.row_start ? c.row_start[c.n_sources] : 0;
+    };
+    const std::uint64_t Ee = edges(d.exc_primary), Ei = edges(d.inh_primary),
+                        Ea = edges(d.neuron_astro), Es = edges(d.astro_neuron);
+    std::uint64_t b = 0;
+    b += N * (7 * 8 + 4 + 16 + 24) + NA * (7 * 8);  // state, params, STP
+    b += slots * N * 16;                              // snapshots
+    b += (Ee + Ei + Ea) * 16 + (N * 3 + NA) * 12;     // out/in lists + row arrays
+    b += slots * ((Ee + Ei + Ea) / 32 + 2 * N + NA) * 4 + slots * (2 * N + NA) * 4;  // bits+cnt
+    b += Es * 4 + N * 8 + slots * NA * 8 + 2 * N * 8;  // SIC (upper bound), factors, values
+    b += 256 * 64;                                     // alignment slack
+    (void)chunk_steps;
+    *bytes = b;
+    return ASG_OK;
+}
+
+int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int64_t first,
+                std::int64_t end, bool keep_spikes, int* id_out) {
+    const std::uint32_t NE = d.n_exc, NI = d.n_inh, N = NE + NI, NA = d.n_astro;
+    if (d.dt <= 0.0) return fail(ASG_ERR_ARG, "dt must be positive");
+    if (d.substeps < 1) return fail(ASG_ERR_ARG, "substeps must be at least 1");
+    if (d.sic_interval < 1) return fail(ASG_ERR_ARG, "sic_interval must be at least 1");
+    if (!delay_ok(d.d_e_steps) || !delay_ok(d.d_i_steps) || !delay_ok(d.d_a2n_steps))
+        return fail(ASG_ERR_ARG, "delays must be at least one step");
+    if (NA >= (1u << 24)) return fail(ASG_ERR_UNSUPPORTED, "at most 2^24-1 astrocytes");
+    if (N > 0 && (d.V_reset == nullptr || d.b == nullptr))
+        return fail(ASG_ERR_ARG, "per-cell V_reset and b are required");
+    if (first < 0 || end < first) return fail(ASG_ERR_ARG, "bad step range");
+    ASG_TRY(check_csr("exc_primary", d.exc_primary, NE, N));
+    ASG_TRY(check_csr("inh_primary", d.inh_primary, NI, N));
+    ASG_TRY(check_csr("neuron_astro", d.neuron_astro, NE, std::max(NA, 1u)));
+    ASG_TRY(check_csr("astro_neuron", d.astro_neuron, NA, N));
+    if (NA == 0 && d.neuron_astro.n_sources && d.neuron_astro.row_start &&
+        d.neuron_astro.row_start[NE] > 0)
+        return fail(ASG_ERR_ARG, "neuron_astro has edges but there are no astrocytes");
+    ASG_TRY(check_uniform("exc_primary", d.exc_primary, NE, d.w_e, d.d_e_steps, d.stp));
+    ASG_TRY(check_uniform("inh_primary", d.inh_primary, NI, d.w_i, d.d_i_steps, d.stp));
+    ASG_TRY(check_uniform("neuron_astro", d.neuron_astro, NE, d.w_n2a, d.d_e_steps, d.stp));
+    asg_stp nostp{};
+    ASG_TRY(check_uniform("astro_neuron", d.astro_neuron, NA, d.w_a2n, d.d_a2n_steps, nostp));
+
+    auto inst = std::make_unique<Instance>();
+    Instance& I = *inst;
+    InstDev& D = I.dev;
+    std::memset(&D, 0, sizeof D);
+    D.N = N;
+    D.NE = NE;
+    D.NA = NA;
+    D.d_e = d.d_e_steps;
+    D.d_i = d.d_i_steps;
+    D.d_a2n = d.d_a2n_steps;
+    D.slots = std::max({1, D.d_e, D.d_i, D.d_a2n}) + 1;
+    D.sic_interval = d.sic_interval;
+    D.fused_sic = cfg.sic_mode == 1 ? 1 : cfg.sic_mode == 2 ? (D.d_a2n >= 2 ? 0 : 1)
+                                                            : (D.d_a2n >= 2 ? 0 : 1);
+    D.stp_on = d.stp.enabled != 0;
+    D.seed = d.seed;
+    D.dt = d.dt;
+    const double h = d.dt / static_cast<double>(d.substeps);
+    D.pe = make_neuron_k(d.exc, d.input_exc, d.dt, h);
+    D.pi = make_neuron_k(d.inh, d.input_inh, d.dt, h);
+    D.ak = make_astro_k(d.astro, h, d.substeps);
+    D.a_rate = d.input_astro.poiss_rate;
+    D.a_weight = d.input_astro.poiss_weight;
+    D.a_lambda = d.input_astro.poiss_rate * d.dt * 1e-3;
+    D.a_limit = std::exp(-D.a_lambda);
+    D.a_std = d.input_astro.gauss_noise_std;
+    D.a_indep = d.input_astro.independent_noise != 0;
+    D.a_steps_per_noise =
+        std::max(1, static_cast<int>(std::llround(d.input_astro.noise_dt / d.dt)));
+    D.SIC_scale = d.astro.SIC_scale;
+    D.SIC_th = d.astro.SIC_th;
+    D.w_e = d.w_e;
+    D.w_i = d.w_i;
+    D.w_n2a = d.w_n2a;
+    D.w_a2n = d.w_a2n;
+    D.U = d.stp.U;
+    D.tau_rec = d.stp.tau_rec;
+    D.tau_fac = d.stp.tau_fac;
+
+    // Per-cell astrocyte parameters collapse to scalars when all equal.
+    const double* pa[4] = {d.Ca_tot, d.IP3_0, d.tau_IP3, d.delta_IP3};
+    const double pu[4] = {d.Ca_tot_u, d.IP3_0_u, d.tau_IP3_u, d.delta_IP3_u};
+    bool uniform = true;
+    double uval[4];
+    for (int k = 0; k < 4; ++k) {
+        if (pa[k] == nullptr) {
+            uval[k] = pu[k];
+        } else if (NA > 0 && all_equal(pa[k], NA)) {
+            uval[k] = pa[k][0];
+        } else if (NA > 0) {
+            uniform = false;
+            uval[k] = 0.0;
+        } else {
+            uval[k] = pu[k];
+        }
+    }
+    D.astro_uniform = uniform ? 1 : 0;
+    D.Ca_tot_u = uval[0];
+    D.IP3_0_u = uval[1];
+    D.tau_u = uval[2];
+    D.delta_u = uval[3];
+
+    // Host preprocessing of the tables.
+    static const std::uint32_t zero_rs[1] = {0};
+    auto rs_of = [](const asg_csr& c) { return c.n_sources ? c.row_start : zero_rs; };
+    InRingHost rex = make_in_ring(NE, rs_of(d.exc_primary), d.exc_primary.target, N);
+    InRingHost rin = make_in_ring(NI, rs_of(d.inh_primary), d.inh_primary.target, N);
+    InRingHost ras = make_in_ring(NE, rs_of(d.neuron_astro), d.neuron_astro.target, NA);
+    SicHost sic = make_sic(NA, rs_of(d.astro_neuron), d.astro_neuron.target, N);
+
+    // Initial state (reference defaults where not given).
+    std::vector<double> V0, Ca0, IP30, h0, stp_x(N, 1.0), stp_u(N, d.stp.U), stp_t(N, -1e12);
+    if (d.V == nullptr) {
+        V0.resize(N);
+        for (std::uint32_t i = 0; i < N; ++i) V0[i] = i < NE ? d.V_m_init_exc : d.V_m_init_inh;
+    }
+    if (d.Ca == nullptr) Ca0.assign(NA, d.Ca_init);
+    if (d.IP3 == nullptr) IP30.assign(NA, d.IP3_init);
+    if (d.h == nullptr) h0.assign(NA, d.h_init);
+    // Per-source STP from the first edge of each row, if the caller gave state.
+    auto take_stp = [&](const asg_csr& c, std::uint32_t n_src, std::uint32_t off) {
+        if (!d.stp.enabled || n_src == 0) return;
+        for (std::uint32_t s = 0; s < n_src; ++s) {
+            const std::uint32_t e = c.row_start[s];
+            if (e == c.row_start[s + 1]) continue;
+            if (c.stp_x) stp_x[off + s] = c.stp_x[e];
+            if (c.stp_u) stp_u[off + s] = c.stp_u[e];
+            if (c.stp_t_last) stp_t[off + s] = c.stp_t_last[e];
+        }
+    };
+    take_stp(d.neuron_astro, NE, 0);
+    take_stp(d.exc_primary, NE, 0);
+    take_stp(d.inh_primary, NI, NE);
+
+    const std::size_t S = static_cast<std::size_t>(D.slots);
+    const std::size_t n8 = static_cast<std::size_t>(N) * 8, a8 = static_cast<std::size_t>(NA) * 8;
+    auto e4 = [](const asg_csr& c) {
+        return static_cast<std::size_t>(c.n_sources ? c.row_start[c.n_sources] : 0) * 4;
+    };
+    std::vector<Seg> segs;
+    auto add_seg = [&](auto*& dst, std::size_t bytes, const void* src) {
+        segs.push_back(Seg{static_cast<void*>(&dst), bytes, src});
+    };
+    add_seg(D.V, n8, d.V ? d.V : V0.data());
+    add_seg(D.w, n8, d.w);
+    add_seg(D.gex, n8, d.g_ex);
+    add_seg(D.dgex, n8, d.dg_ex);
+    add_seg(D.gin, n8, d.g_in);
+    add_seg(D.dgin, n8, d.dg_in);
+    add_seg(D.Isic, n8, d.I_sic);
+    add_seg(D.refr, static_cast<std::size_t>(N) * 4, d.refractory);
+    add_seg(D.V_reset, n8, d.V_reset);
+    add_seg(D.b, n8, d.b);
+    add_seg(D.Ca, a8, d.Ca ? d.Ca : Ca0.data());
+    add_seg(D.IP3, a8, d.IP3 ? d.IP3 : IP30.data());
+    add_seg(D.h, a8, d.h ? d.h : h0.data());
+    if (!uniform) {
+        add_seg(D.Ca_tot, a8, d.Ca_tot);
+        add_seg(D.IP3_0, a8, d.IP3_0);
+        add_seg(D.tau, a8, d.tau_IP3);
+        add_seg(D.delta, a8, d.delta_IP3);
+    }
+    add_seg(D.stp_x, n8, stp_x.data());
+    add_seg(D.stp_u, n8, stp_u.data());
+    add_seg(D.stp_t, n8, stp_t.data());
+    add_seg(D.snap_x, S * n8, nullptr);
+    add_seg(D.snap_u, S * n8, nullptr);
+    add_seg(D.exc_rs, (NE + 1) * 4, d.exc_primary.n_sources ? d.exc_primary.row_start : zero_rs);
+    add_seg(D.exc_tg, e4(d.exc_primary), d.exc_primary.target);
+    add_seg(D.inh_rs, (NI + 1) * 4, d.inh_primary.n_sources ? d.inh_primary.row_start : zero_rs);
+    add_seg(D.inh_tg, e4(d.inh_primary), d.inh_primary.target);
+    add_seg(D.n2a_rs, (NE + 1) * 4, d.neuron_astro.n_sources ? d.neuron_astro.row_start : zero_rs);
+    add_seg(D.n2a_tg, e4(d.neuron_astro), d.neuron_astro.target);
+    auto ring_segs = [&](InRing& R, InRingHost& H, std::uint32_t n_t) {
+        add_seg(R.row, H.row.size() * 4, H.row.data());
+        add_seg(R.src, H.src.size() * 4, H.src.data());
+        add_seg(R.wbase, H.wbase.size() * 4, H.wbase.data());
+        add_seg(R.bitpos, H.bitpos.size() * 4, H.bitpos.data());
+        add_seg(R.bits, S * std::max<std::uint32_t>(H.words, 1) * 4, nullptr);
+        add_seg(R.cnt, S * std::max<std::uint32_t>(n_t, 1) * 4, nullptr);
+        R.words = H.words;
+        R.n_targets = n_t;
+    };
+    ring_segs(D.ring_ex, rex, N);
+    ring_segs(D.ring_in, rin, N);
+    ring_segs(D.ring_as, ras, NA);
+    add_seg(D.sic_soff, sic.soff.size() * 4, sic.soff.data());
+    add_seg(D.sic_ent, sic.ent.size() * 4, sic.ent.data());
+    add_seg(D.fac, S * std::max<std::size_t>(a8, 8), nullptr);
+    add_seg(D.sic_val, 2 * std::max<std::size_t>(n8, 8), nullptr);
+
+    std::size_t total = 0;
+    for (const Seg& s : segs) total += align256(std::max<std::size_t>(s.bytes, 1));
+    if (resident_bytes + total > cfg.mem_budget)
+        return fail(ASG_ERR_OOM, "instance needs %zu device bytes; %llu of %llu in use", total,
+                    static_cast<unsigned long long>(resident_bytes),
+                    static_cast<unsigned long long>(cfg.mem_budget));
+    ASG_TRY(I.arena.alloc(total, false));
+    I.arena_bytes = total;
+    {
+        char* base = I.arena.as<char>();
+        std::size_t off = 0;
+        std::vector<char> zeros;
+        for (const Seg& s : segs) {
+            *static_cast<void**>(s.dst) = base + off;
+            if (s.bytes > 0) {
+                if (s.src != nullptr) {
+                    ASG_CUDA(cudaMemcpyAsync(base + off, s.src, s.bytes, cudaMemcpyHostToDevice,
+                                             stream));
+                } else {
+                    ASG_CUDA(cudaMemsetAsync(base + off, 0, s.bytes, stream));
+                }
+            }
+            off += align256(std::max<std::size_t>(s.bytes, 1));
+        }
+        ASG_CUDA(cudaStreamSynchronize(stream));  // host sources go out of scope
+    }
+
+    // Recording and spike-log buffers (mapped host memory, two parities).
+    asg_record_opts ro{};
+    if (rec) ro = *rec;
+    if (ro.record_every < 1) ro.record_every = 1;
+    D.rec_spikes = ro.spikes ? 1 : 0;
+    D.rec_from = ro.record_from_step;
+    D.rec_every = ro.record_every;
+    D.rec_astro_max = std::min(ro.astro_max, NA);
+    D.rec_neuron_max = std::min(ro.neuron_max, N);
+    I.rec_rows = static_cast<std::uint32_t>(cfg.chunk_steps / ro.record_every + 2);
+    D.rec_rows = I.rec_rows;
+    const std::uint64_t full = static_cast<std::uint64_t>(N) * cfg.chunk_steps;
+    I.log_cap = static_cast<std::uint32_t>(
+        std::max<std::uint64_t>(1, std::min<std::uint64_t>(full, std::max<std::uint64_t>(
+                                                                     65536, full / 8))));
+    I.keep_spikes = keep_spikes;
+    const std::size_t rec_doubles =
+        static_cast<std::size_t>(I.rec_rows) * (2 * D.rec_astro_max + 2 * D.rec_neuron_max) + 1;
+    for (int p = 0; p < 2; ++p) {
+        if (D.rec_spikes) {
+            ASG_CUDA(cudaHostAlloc(&I.log_h[p], static_cast<std::size_t>(I.log_cap) * 8,
+                                   cudaHostAllocMapped));
+            ASG_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&I.log_d[p]), I.log_h[p], 0));
+        }
+        ASG_CUDA(cudaHostAlloc(&I.rec_h[p], rec_doubles * 8, cudaHostAllocMapped));
+        ASG_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&I.rec_d[p]), I.rec_h[p], 0));
+    }
+    D.spike_log_cap = D.rec_spikes ? I.log_cap : 0;
+    I.step = first;
+    I.end = end;
+    I.id = next_id++;
+    resident_bytes += total;
+    *id_out = I.id;
+    insts.push_back(std::move(inst));
+    dirty = true;
+    return ASG_OK;
+}
+
+int Engine::remove(int id) {
+    ASG_TRY(finish_pending());  // pending statistics are indexed by position
+    for (std::size_t i = 0; i < insts.size(); ++i) {
+        if (insts[i]->id == id) {
+            ASG_CUDA(cudaStreamSynchronize(stream));
+            resident_bytes -= insts[i]->arena_bytes;
+            insts.erase(insts.begin() + static_cast<std::ptrdiff_t>(i));
+            dirty = true;
+            return ASG_OK;
+        }
+    }
+    return fail(ASG_ERR_NOT_FOUND, "no instance %d", id);
+}
+
+int Engine::set_block(int block) {
+    if (block < 32 || block > 512 || block % 32)
+        return fail(ASG_ERR_ARG, "block size %d must be a multiple of 32 in [32, 512]", block);
+    cfg.block = block;
+    dirty = true;
+    return ASG_OK;
+}
+
+int Engine::set_chunk(int chunk) {
+    if (chunk < 1) return fail(ASG_ERR_ARG, "chunk must be >= 1");
+    // Record rings are sized by the chunk at add(); keep chunks within them.
+    for (auto& p : insts)
+        if (static_cast<std::uint32_t>(chunk / p->dev.rec_every + 2) > p->rec_rows ||
+            static_cast<std::uint64_t>(chunk) * p->dev.N > 8ull * p->log_cap + 65536ull * 8)
+            return fail(ASG_ERR_ARG, "chunk %d exceeds the output buffers sized at creation",
+                        chunk);
+    cfg.chunk_steps = chunk;
+    dirty = true;
+    return ASG_OK;
+}
+
+int Engine::rebuild() {
+    ASG_TRY(finish_pending());
+    ASG_CUDA(cudaStreamSynchronize(stream));
+    if (graph) {
+        cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
+    const int B = cfg.block;
+    work.clear();
+    order.clear();
+    // SIC blocks first (longest dependent chains), then neurons, then astrocytes.
+    for (int role = 0; role < 3; ++role) {
+        for (std::size_t s = 0; s < insts.size(); ++s) {
+            const InstDev& D = insts[s]->dev;
+            const std::uint16_t r = role == 0 ? kRoleSic : role == 1 ? kRoleNeuron : kRoleAstro;
+            if (r == kRoleSic && D.fused_sic) continue;
+            const std::uint32_t n = r == kRoleAstro ? D.NA : D.N;
+            for (std::uint32_t f = 0; f < n; f += B)
+                work.push_back(Work{static_cast<std::uint32_t>(s), r, 0, f,
+                                    std::min<std::uint32_t>(B, n - f)});
+        }
+    }
+    if (insts.size() > cap_insts || work.size() * sizeof(Work) > d_work.bytes()) {
+        const std::size_t cap = std::max<std::size_t>(insts.size(), 1);
+        if (cap > cap_insts) {
+            const std::size_t c2 = std::max(cap, cap_insts * 2);
+            ASG_TRY(d_insts.alloc(c2 * sizeof(InstDev)));
+            ASG_TRY(d_stats.alloc(c2 * 8 * sizeof(unsigned long long)));
+            for (int p = 0; p < 2; ++p) {
+                if (h_insts[p]) cudaFreeHost(h_insts[p]);
+                if (h_stats[p]) cudaFreeHost(h_stats[p]);
+                h_insts[p] = nullptr;
+                h_stats[p] = nullptr;
+                ASG_CUDA(cudaHostAlloc(&h_insts[p], c2 * sizeof(InstDev), cudaHostAllocDefault));
+                ASG_CUDA(cudaHostAlloc(&h_stats[p], c2 * 8 * sizeof(unsigned long long),
+                                       cudaHostAllocDefault));
+            }
+            cap_insts = c2;
+        }
+        if (work.size() * sizeof(Work) > d_work.bytes())
+            ASG_TRY(d_work.alloc(std::max<std::size_t>(work.size(), 64) * 2 * sizeof(Work)));
+    }
+    if (!work.empty())
+        ASG_CUDA(cudaMemcpyAsync(d_work.get(), work.data(), work.size() * sizeof(Work),
+                                 cudaMemcpyHostToDevice, stream));
+    ASG_CUDA(cudaMemsetAsync(d_stats.get(), 0, cap_insts * 8 * sizeof(unsigned long long), stream));
+    ASG_CUDA(cudaStreamSynchronize(stream));
+    graph_steps = 0;
+    if (cfg.use_graphs >= 0 && !work.empty()) {
+        cudaGraph_t g = nullptr;
+        ASG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < cfg.chunk_steps; ++k)
+            launch_step(d_insts.as<InstDev>(), d_work.as<Work>(), static_cast<int>(work.size()),
+                        B, k, stream);
+        const cudaError_t ce = cudaStreamEndCapture(stream, &g);
+        if (ce != cudaSuccess) return cuda_fail(ce, "graph capture", __FILE__, __LINE__);
+        const cudaError_t ci = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ci != cudaSuccess) return cuda_fail(ci, "graph instantiate", __FILE__, __LINE__);
+        graph_steps = cfg.chunk_steps;
+    }
+    dirty = false;
+    return ASG_OK;
+}
+
+int Engine::launch_chunk(int parity, int steps) {
+    // Stage the descriptors: step window of this chunk, output pointers.
+    InstDev* hi = h_insts[parity];
+    for (std::size_t s = 0; s < insts.size(); ++s) {
+        Instance& I = *insts[s];
+        InstDev D = I.dev;
+        D.step0 = I.step;
+        D.end_step = std::min<std::int64_t>(I.end, I.step + steps);
+        unsigned long long* st = d_stats.as<unsigned long long>() + s * 8;
+        D.spike_log_n = st;
+        D.counters = st + 1;
+        D.spike_log = I.log_d[parity];
+        double* r = I.rec_d[parity];
+        const std::size_t R = I.rec_rows;
+        D.rec_Ca = r;
+        D.rec_IP3 = r + R * D.rec_astro_max;
+        D.rec_V = r + 2 * R * D.rec_astro_max;
+        D.rec_Isic = r + 2 * R * D.rec_astro_max + R * D.rec_neuron_max;
+        hi[s] = D;
+        I.chunk_first[parity] = I.step;
+        I.chunk_last[parity] = D.end_step;
+    }
+    ASG_CUDA(cudaMemcpyAsync(d_insts.get(), hi, insts.size() * sizeof(InstDev),
+                             cudaMemcpyHostToDevice, stream));
+    if (graph != nullptr && steps == graph_steps) {
+        ASG_CUDA(cudaGraphLaunch(graph, stream));
+    } else {
+        for (int k = 0; k < steps; ++k)
+            launch_step(d_insts.as<InstDev>(), d_work.as<Work>(), static_cast<int>(work.size()),
+                        cfg.block, k, stream);
+        ASG_CUDA(cudaGetLastError());
+    }
+    last_kernels += steps;
+    ASG_CUDA(cudaMemcpyAsync(h_stats[parity], d_stats.get(),
+                             insts.size() * 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             stream));
+    ASG_CUDA(cudaMemsetAsync(d_stats.get(), 0, insts.size() * 8 * sizeof(unsigned long long),
+                             stream));
+    ASG_CUDA(cudaEventRecord(ev_chunk[parity], stream));
+    pending[parity] = true;
+    for (auto& p : insts) p->step = std::min<std::int64_t>(p->end, p->step + steps);
+    return ASG_OK;
+}
+
+int Engine::collect(int parity) {
+    if (!pending[parity]) return ASG_OK;
+    ASG_CUDA(cudaEventSynchronize(ev_chunk[parity]));
+    pending[parity] = false;
+    const unsigned long long* st = h_stats[parity];
+    for (std::size_t s = 0; s < insts.size(); ++s) {
+        Instance& I = *insts[s];
+        const InstDev& D = I.dev;
+        const unsigned long long* c = st + s * 8;
+        if (c[4] != 0)
+            return fail(ASG_ERR_OVERFLOW,
+                        "instance %d: %llu spikes did not fit the %u-entry chunk log; use a "
+                        "smaller chunk_steps",
+                        I.id, c[4], I.log_cap);
+        I.spike_edges += static_cast<std::int64_t>(c[1]);
+        I.sic_edges += static_cast<std::int64_t>(c[2]);
+        I.n_spikes += static_cast<std::int64_t>(c[3]);
+        if (D.rec_spikes && I.keep_spikes) {
+            const std::uint64_t n = std::min<std::uint64_t>(c[0], I.log_cap);
+            const unsigned long long* lg = I.log_h[parity];
+            const std::size_t base = I.spikes.size();
+            I.spikes.resize(base + n);
+            for (std::uint64_t q = 0; q < n; ++q)
+                I.spikes[base + q] = SpikeRec{static_cast<std::int64_t>(lg[q] >> 32),
+                                              static_cast<std::uint32_t>(lg[q] & 0xFFFFFFFFu)};
+            std::sort(I.spikes.begin() + static_cast<std::ptrdiff_t>(base), I.spikes.end(),
+                      [](const SpikeRec& a, const SpikeRec& b) {
+                          return a.step != b.step ? a.step < b.step : a.source < b.source;
+                      });
+        }
+        // Record rows written in this chunk.
+        const std::int64_t f = I.chunk_first[parity], l = I.chunk_last[parity];
+        if ((D.rec_astro_max || D.rec_neuron_max) && l > f) {
+            const std::size_t R = I.rec_rows;
+            const double* r = I.rec_h[parity];
+            for (std::int64_t s2 = std::max<std::int64_t>(f, D.rec_from); s2 < l; ++s2) {
+                if ((s2 - D.rec_from) % D.rec_every != 0) continue;
+                const std::size_t row = static_cast<std::size_t>(((s2 - D.rec_from) / D.rec_every) % R);
+                if (D.rec_astro_max) {
+                    I.astro_rec_steps.push_back(s2);
+                    const double* ca = r + row * D.rec_astro_max;
+                    const double* ip = r + R * D.rec_astro_max + row * D.rec_astro_max;
+                    I.rec_Ca.insert(I.rec_Ca.end(), ca, ca + D.rec_astro_max);
+                    I.rec_IP3.insert(I.rec_IP3.end(), ip, ip + D.rec_astro_max);
+                }
+                if (D.rec_neuron_max) {
+                    I.neuron_rec_steps.push_back(s2);
+                    const double* v = r + 2 * R * D.rec_astro_max + row * D.rec_neuron_max;
+                    const double* is = r + 2 * R * D.rec_astro_max + R * D.rec_neuron_max +
+                                       row * D.rec_neuron_max;
+                    I.rec_V.insert(I.rec_V.end(), v, v + D.rec_neuron_max);
+                    I.rec_Isic.insert(I.rec_Isic.end(), is, is + D.rec_neuron_max);
+                }
+            }
+        }
+    }
+    return ASG_OK;
+}
+
+int Engine::finish_pending() {
+    for (int k = 0; k < 2; ++k) ASG_TRY(collect((next_parity + k) & 1));
+    return ASG_OK;
+}
+
+int Engine::run_chunk(std::int64_t max_steps) {
+    if (dirty) ASG_TRY(rebuild());
+    std::int64_t steps = 0;
+    for (auto& p : insts) steps = std::max<std::int64_t>(steps, p->end - p->step);
+    steps = std::min<std::int64_t>({steps, max_steps, cfg.chunk_steps});
+    if (steps <= 0 || work.empty()) return ASG_OK;
+    // Two chunks in flight: the host collects one while the next runs.
+    const int p = next_parity;
+    ASG_TRY(collect(p));
+    ASG_TRY(launch_chunk(p, static_cast<int>(steps)));
+    next_parity ^= 1;
+    ++chunks;
+    return ASG_OK;
+}
+
+int Engine::run(std::int64_t n_steps) {
+    if (n_steps < 0) return fail(ASG_ERR_ARG, "negative step count");
+    if (dirty) ASG_TRY(rebuild());
+    last_kernels = 0;
+    std::vector<std::int64_t> target(insts.size());
+    for (std::size_t s = 0; s < insts.size(); ++s)
+        target[s] = std::min<std::int64_t>(insts[s]->end, insts[s]->step + n_steps);
+    // Restrict every instance to this call's window.
+    std::vector<std::int64_t> saved_end(insts.size());
+    for (std::size_t s = 0; s < insts.size(); ++s) {
+        saved_end[s] = insts[s]->end;
+        insts[s]->end = target[s];
+    }
+    ASG_CUDA(cudaEventRecord(ev_start, stream));
+    int st = ASG_OK;
+    for (;;) {
+        bool any = false;
+        for (auto& p : insts) any = any || !p->done();
+        if (!any) break;
+        st = run_chunk(cfg.chunk_steps);
+        if (st != ASG_OK) break;
+    }
+    if (st == ASG_OK) st = finish_pending();
+    for (std::size_t s = 0; s < insts.size(); ++s) insts[s]->end = saved_end[s];
+    ASG_TRY(st);
+    ASG_CUDA(cudaEventRecord(ev_end, stream));
+    ASG_CUDA(cudaEventSynchronize(ev_end));
+    float ms = 0.0f;
+    ASG_CUDA(cudaEventElapsedTime(&ms, ev_start, ev_end));
+    last_ms = ms;
+    total_ms += ms;
+    total_kernels += last_kernels;
+    return ASG_OK;
+}
+
+int Engine::pull_state(int id, asg_state* out) {
+    Instance* I = find(id);
+    if (I == nullptr) return fail(ASG_ERR_NOT_FOUND, "no instance %d", id);
+    ASG_TRY(finish_pending());
+    const InstDev& D = I->dev;
+    const std::size_t n8 = static_cast<std::size_t>(D.N) * 8, a8 = static_cast<std::size_t>(D.NA) * 8;
+    struct {
+        void* dst;
+        const void* src;
+        std::size_t bytes;
+    } cp[] = {{out->V, D.V, n8},       {out->w, D.w, n8},         {out->g_ex, D.gex, n8},
+              {out->dg_ex, D.dgex, n8}, {out->g_in, D.gin, n8},    {out->dg_in, D.dgin, n8},
+              {out->I_sic, D.Isic, n8}, {out->refractory, D.refr, static_cast<std::size_t>(D.N) * 4},
+              {out->Ca, D.Ca, a8},      {out->IP3, D.IP3, a8},     {out->h, D.h, a8}};
+    for (auto& c : cp)
+        if (c.dst && c.bytes)
+            ASG_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, stream));
+    ASG_CUDA(cudaStreamSynchronize(stream));
+    return ASG_OK;
+}
+
+int Engine::pull_stp(int id, double* x, double* u, double* t) {
+    Instance* I = find(id);
+    if (I == nullptr) return fail(ASG_ERR_NOT_FOUND, "no instance %d", id);
+    ASG_TRY(finish_pending());
+    const std::size_t n8 = static_cast<std::size_t>(I->dev.N) * 8;
+    if (n8 == 0) return ASG_OK;
+    if (x) ASG_CUDA(cudaMemcpyAsync(x, I->dev.stp_x, n8, cudaMemcpyDeviceToHost, stream));
+    if (u) ASG_CUDA(cudaMemcpyAsync(u, I->dev.stp_u, n8, cudaMemcpyDeviceToHost, stream));
+    if (t) ASG_CUDA(cudaMemcpyAsync(t, I->dev.stp_t, n8, cudaMemcpyDeviceToHost, stream));
+    ASG_CUDA(cudaStreamSynchronize(stream));
+    return ASG_OK;
+}
+
+}  // namespace asg

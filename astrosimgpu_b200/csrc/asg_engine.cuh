@@ -1,0 +1,126 @@
+// Device data layout of the network engine (one descriptor per instance) and
+// the fused per-timestep kernel.
+//
+// One kernel launch advances every resident instance by one step.  Its
+// blocks are typed by a work table built on the host:
+//   NEURON  arrivals (exc/inh rings, SIC), Poisson drive, noise, AdEx RK4,
+//           spike test, STP update of the spiking source and the push of its
+//           out-edges into the arrival rings of later steps;
+//   ASTRO   arrivals (neuron->astrocyte ring), Poisson drive, noise, Li-Rinzel
+//           RK4, SIC factor of the step;
+//   SIC     (only when the SIC delay is >= 2 steps) the SIC current arriving
+//           at the NEXT step, summed from the factors of its emission step.
+// No role waits on another inside a launch: every cross-cell read is of data
+// written by an earlier launch (delays are >= 1 step), so one launch per step
+// is the only synchronisation, and K steps are one captured CUDA graph.
+//
+// Exact, reproducible arrivals without floating-point atomics
+// ----------------------------------------------------------
+// The reference sums each ring entry sequentially in ascending source order
+// (network.cpp:249-279).  Here every target owns one bit per incoming edge,
+// its in-edges sorted by (source, position in the source's row).  A spiking
+// source sets the bits of its out-edges in the arrival slot (integer
+// atomicOr, no return value needed) and bumps the target's pending count.
+// The target, when that slot arrives, walks its set bits in ascending order
+// and adds the contributions left to right: the same IEEE operations in the
+// same order as the reference, hence bitwise equal, for any number of
+// coincident spikes.
+//
+// STP: the reference keeps x, u, t_last per edge, but all edges of a source
+// start equal (network.cpp:43-52) and are updated together on each spike of
+// that source, so they stay equal: one state per source is exact.  The
+// spiking thread updates it and stores the post-spike (x, u) in a snapshot
+// row of its emission slot, from which the receivers form w*x*u.
+//
+// SIC: the reference adds w_a2n*factor(a) once per astrocyte->neuron edge, in
+// ascending astrocyte order (network.cpp:281-299).  A target's edges from one
+// astrocyte all add the same value, so its list is stored compressed as
+// (astrocyte, multiplicity) pairs in ascending astrocyte order and summed
+// sequentially -- same operations, far fewer bytes.  Layout: sliced ELL with
+// slices of 32 targets (one warp), entries packed as astro << 8 | mult.
+#pragma once
+
+#include <cstdint>
+
+#include "asg_device.cuh"
+
+namespace asg {
+
+enum Role : std::uint16_t { kRoleNeuron = 0, kRoleAstro = 1, kRoleSic = 2 };
+
+struct Work {
+    std::uint32_t inst;
+    std::uint16_t role;
+    std::uint16_t pad;
+    std::uint32_t first;
+    std::uint32_t count;
+};
+
+// Incoming-edge structure of one arrival ring (transpose of a source CSR).
+struct InRing {
+    const std::uint32_t* row;     // [n_targets+1] start of each target's in-list
+    const std::uint32_t* src;     // [E] source of each in-edge (sorted per target)
+    const std::uint32_t* wbase;   // [n_targets+1] first bitmap word of each target
+    const std::uint32_t* bitpos;  // [E] bit index of each OUT-edge (source CSR order)
+    std::uint32_t* bits;          // [slots][total words] arrival bitmaps
+    std::uint32_t* cnt;           // [slots][n_targets] set bits pending per target
+    std::uint32_t words;          // total bitmap words of one slot
+    std::uint32_t n_targets;
+};
+
+struct InstDev {
+    // sizes and time
+    std::uint32_t N, NE, NA;
+    std::int32_t slots, d_e, d_i, d_a2n, sic_interval;
+    std::int32_t fused_sic;  // 1: neuron thread sums its own SIC
+    std::int32_t stp_on;
+    std::int64_t step0;      // step of kernel index 0 in the current chunk
+    std::int64_t end_step;   // first step this instance does not run
+    std::uint64_t seed;
+    double dt;
+    // neuron populations
+    NeuronK pe, pi;
+    double sh_std_e, sh_std_i;  // shared-noise std (0 unless shared noise is on)
+    // astrocytes
+    AstroK ak;
+    std::int32_t astro_uniform;
+    double Ca_tot_u, IP3_0_u, tau_u, delta_u;
+    double a_rate, a_weight, a_lambda, a_limit, a_std;
+    std::int32_t a_indep, a_steps_per_noise;
+    double SIC_scale, SIC_th;
+    // synapses
+    double w_e, w_i, w_n2a, w_a2n, U, tau_rec, tau_fac;
+    // neuron state
+    double *V, *w, *gex, *dgex, *gin, *dgin, *Isic;
+    std::int32_t* refr;
+    const double *V_reset, *b;
+    // astrocyte state / params
+    double *Ca, *IP3, *h;
+    const double *Ca_tot, *IP3_0, *tau, *delta;
+    // STP per source + per-slot snapshots of (x, u) at emission
+    double *stp_x, *stp_u, *stp_t;
+    double *snap_x, *snap_u;  // [slots][N]
+    // out-edge CSR (source order) of the three spike-carrying sets
+    const std::uint32_t *exc_rs, *exc_tg, *inh_rs, *inh_tg, *n2a_rs, *n2a_tg;
+    InRing ring_ex, ring_in, ring_as;
+    // SIC: sliced ELL over targets, factors per emission slot, split values
+    const std::uint32_t* sic_soff;  // [n_slices+1] entry offset of each 32-target slice
+    const std::uint32_t* sic_ent;   // astro << 8 | mult
+    double* fac;                    // [slots][NA]
+    double* sic_val;                // [2][N]
+    // outputs (host-mapped memory)
+    unsigned long long* spike_log;  // (step << 32) | source
+    unsigned long long* spike_log_n;
+    std::uint32_t spike_log_cap;
+    std::int32_t rec_spikes;
+    std::int64_t rec_from;
+    std::int32_t rec_every;
+    std::uint32_t rec_astro_max, rec_neuron_max, rec_rows;  // rows held in the ring below
+    double *rec_Ca, *rec_IP3, *rec_V, *rec_Isic;             // [rec_rows][max]
+    unsigned long long* counters;  // spike_edges, sic_edges, spikes, overflow
+};
+
+void launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
+                 cudaStream_t stream);
+
+}  // namespace asg

@@ -1,0 +1,122 @@
+// Host side of the network engine: one Engine holds any number of resident
+// network instances (a plain run is an engine with one instance, a sweep is
+// a batch, serving adds and removes instances at step boundaries) and
+// advances them together, one fused kernel launch per step, K steps per
+// captured CUDA graph ("chunk").
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "asg_b200.h"
+#include "asg_common.hpp"
+#include "asg_engine.cuh"
+
+namespace asg {
+
+struct SpikeRec {
+    std::int64_t step;
+    std::uint32_t source;
+};
+
+// One resident instance.
+struct Instance {
+    int id = -1;
+    InstDev dev{};             // host copy of the device descriptor
+    DevBuf arena;              // every device array of the instance
+    std::size_t arena_bytes = 0;
+    std::int64_t step = 0;     // next step to run
+    std::int64_t end = INT64_MAX;
+    bool done() const { return step >= end; }
+    // outputs gathered on the host
+    std::vector<SpikeRec> spikes;
+    std::vector<std::int64_t> astro_rec_steps, neuron_rec_steps;
+    std::vector<double> rec_Ca, rec_IP3, rec_V, rec_Isic;
+    std::int64_t spike_edges = 0, sic_edges = 0, n_spikes = 0;
+    // mapped host buffers for logs and record rows, two per parity
+    unsigned long long* log_h[2] = {nullptr, nullptr};
+    unsigned long long* log_d[2] = {nullptr, nullptr};
+    double* rec_h[2] = {nullptr, nullptr};  // Ca | IP3 | V | Isic rows
+    double* rec_d[2] = {nullptr, nullptr};
+    std::uint32_t log_cap = 0;
+    std::uint32_t rec_rows = 0;
+    std::int64_t chunk_first[2] = {0, 0};   // first step of the chunk written to parity p
+    std::int64_t chunk_last[2] = {0, 0};
+    bool keep_spikes = true;
+    ~Instance();
+};
+
+struct EngineConfig {
+    int device = 0;
+    int chunk_steps = 32;
+    int block = 128;
+    int use_graphs = 1;
+    int sic_mode = 0;  // 0 auto, 1 fused, 2 split
+    std::uint64_t mem_budget = 0;
+};
+
+class Engine {
+public:
+    explicit Engine(const EngineConfig& cfg);
+    ~Engine();
+    int init();
+
+    // Adds an instance from a descriptor; it runs steps [first, end).
+    int add(const asg_network_desc& d, const asg_record_opts* rec, std::int64_t first,
+            std::int64_t end, bool keep_spikes, int* id);
+    int remove(int id);
+    Instance* find(int id);
+    // Bytes an instance of this descriptor would hold on the device.
+    static int footprint(const asg_network_desc& d, int chunk_steps, std::uint64_t* bytes);
+
+    // Runs chunks until every instance advanced by n_steps (or reached its
+    // end).  Outputs are gathered into each Instance.
+    int run(std::int64_t n_steps);
+    // One chunk of up to chunk_steps (serving loop granularity).
+    int run_chunk(std::int64_t max_steps);
+
+    int pull_state(int id, asg_state* out);
+    int pull_stp(int id, double* x, double* u, double* t);
+
+    EngineConfig cfg;
+    std::vector<std::unique_ptr<Instance>> insts;
+    double last_ms = 0.0;
+    std::int64_t last_kernels = 0;
+    double total_ms = 0.0;
+    std::int64_t total_kernels = 0;
+    std::int64_t chunks = 0;
+    std::uint64_t resident_bytes = 0;
+    cudaStream_t stream = nullptr;
+    int sms = 148;
+
+    int set_block(int block);
+    int set_chunk(int chunk);
+
+private:
+    int rebuild();          // work table + graph after the instance set changed
+    int launch_chunk(int parity, int steps);
+    int collect(int parity);
+    int finish_pending();
+
+    DevBuf d_insts, d_work;
+    InstDev* h_insts[2] = {nullptr, nullptr};  // pinned staging
+    unsigned long long* h_stats[2] = {nullptr, nullptr};  // pinned: per inst log_n + counters
+    DevBuf d_stats;        // [n][8]: log_n, spike_edges, sic_edges, spikes, overflow
+    std::size_t cap_insts = 0;
+    std::vector<Work> work;
+    std::vector<int> order;  // instance index per device slot
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    bool dirty = true;
+    cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+    cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
+    bool pending[2] = {false, false};
+    int next_parity = 0;
+    int next_id = 0;
+};
+
+}  // namespace asg

@@ -1,0 +1,357 @@
+// The fused per-timestep kernel of the network engine (layout and design in
+// asg_engine.cuh).  Compiled with -fmad=false: every floating-point
+// expression is evaluated as separate IEEE operations in the reference's
+// order (neuron.cpp:101-250, astrocyte.cpp:233-329, network.cpp:230-355).
+
+#include <cuda_runtime.h>
+
+#include "asg_engine.cuh"
+
+namespace asg {
+
+namespace {
+
+constexpr int kMaxBlock = 512;
+
+// Routes one arrival the way NeuronPopulation::add_synaptic_input does
+// (neuron.cpp:77-83): positive weights to the excitatory input, negative
+// ones (as magnitudes) to the inhibitory input.
+__device__ __forceinline__ void add_syn(double v, double& exc_in, double& inh_in) {
+    if (v > 0.0) {
+        exc_in += v;
+    } else if (v < 0.0) {
+        inh_in -= v;
+    }
+}
+
+// Ordered sum of one target's arrivals in `slot` (see asg_engine.cuh).
+// kSubtract selects ring_inh's `-=` accumulation (network.cpp:271-275).
+template <bool kSubtract>
+__device__ __forceinline__ double ring_sum(const InstDev& I, const InRing& R, int slot,
+                                           std::uint32_t t, std::int64_t emit_step,
+                                           double weight) {
+    std::uint32_t* cnt = R.cnt + static_cast<std::size_t>(slot) * R.n_targets + t;
+    const std::uint32_t n = *cnt;
+    if (n == 0) return 0.0;
+    *cnt = 0;
+    const std::size_t snap = static_cast<std::size_t>(emit_step % I.slots) * I.N;
+    std::uint32_t* bits = R.bits + static_cast<std::size_t>(slot) * R.words;
+    const std::uint32_t w0 = R.wbase[t], w1 = R.wbase[t + 1];
+    const std::uint32_t* src = R.src + R.row[t];
+    double acc = 0.0;
+    std::uint32_t seen = 0;
+    for (std::uint32_t q = w0; q < w1 && seen < n; ++q) {
+        std::uint32_t word = bits[q];
+        if (word == 0) continue;
+        bits[q] = 0;
+        while (word != 0) {
+            const int b = __ffs(word) - 1;
+            word &= word - 1;
+            const std::uint32_t j = src[(q - w0) * 32 + b];
+            const double c = I.stp_on ? weight * I.snap_x[snap + j] * I.snap_u[snap + j] : weight;
+            if (kSubtract) {
+                acc -= c;
+            } else {
+                acc += c;
+            }
+            ++seen;
+        }
+    }
+    return acc;
+}
+
+// Sequential SIC sum of target t from the factors of emission slot fslot
+// (network.cpp:281-299 order: ascending astrocyte, one add per edge).
+__device__ __forceinline__ double sic_sum(const InstDev& I, std::uint32_t t, int fslot,
+                                          unsigned long long& edges) {
+    const std::uint32_t slice = t >> 5, lane = t & 31;
+    const std::uint32_t o0 = I.sic_soff[slice], o1 = I.sic_soff[slice + 1];
+    const std::uint32_t len = (o1 - o0) >> 5;
+    const double* fac = I.fac + static_cast<std::size_t>(fslot) * I.NA;
+    double acc = 0.0;
+    for (std::uint32_t q = 0; q < len; ++q) {
+        const std::uint32_t e = I.sic_ent[o0 + q * 32 + lane];
+        const std::uint32_t m = e & 0xFFu;
+        if (m == 0) break;  // padding ends the list
+        const double f = fac[e >> 8];
+        if (f == 0.0) continue;
+        const double c = I.w_a2n * f;
+        for (std::uint32_t r = 0; r < m; ++r) acc += c;
+        edges += m;
+    }
+    return acc;
+}
+
+__device__ __forceinline__ void push_row(const std::uint32_t* rs, const std::uint32_t* tg,
+                                         const InRing& R, std::uint32_t row, int slot) {
+    std::uint32_t* bits = R.bits + static_cast<std::size_t>(slot) * R.words;
+    std::uint32_t* cnt = R.cnt + static_cast<std::size_t>(slot) * R.n_targets;
+    const std::uint32_t e1 = rs[row + 1];
+#pragma unroll 4
+    for (std::uint32_t e = rs[row] + threadIdx.x; e < e1; e += blockDim.x) {
+        const std::uint32_t t = tg[e];
+        const std::uint32_t b = R.bitpos[e];
+        atomicOr(bits + (b >> 5), 1u << (b & 31));
+        atomicAdd(cnt + t, 1u);
+    }
+}
+
+__device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step) {
+    __shared__ std::uint32_t s_spk[kMaxBlock];
+    __shared__ int s_nspk;
+    if (threadIdx.x == 0) s_nspk = 0;
+    __syncthreads();
+
+    const std::uint32_t c = wk.first + threadIdx.x;
+    if (threadIdx.x < wk.count) {
+        const bool exc = c < I.NE;
+        const NeuronK& P = exc ? I.pe : I.pi;
+        const int slot = static_cast<int>(step % I.slots);
+
+        // apply_arrivals (network.cpp:301-338)
+        double exc_in = 0.0, inh_in = 0.0;
+        {
+            const double ex = ring_sum<false>(I, I.ring_ex, slot, c, step - I.d_e, I.w_e);
+            if (ex != 0.0) add_syn(ex, exc_in, inh_in);
+            const double in = ring_sum<true>(I, I.ring_in, slot, c, step - I.d_i, I.w_i);
+            if (in != 0.0) add_syn(-in, exc_in, inh_in);
+        }
+        double Isic = I.Isic[c];
+        const std::int64_t se = step - I.d_a2n;
+        if (se >= 0 && se % I.sic_interval == 0) {
+            if (I.fused_sic) {
+                unsigned long long edges = 0;
+                Isic = sic_sum(I, c, static_cast<int>(se % I.slots), edges);
+                if (edges) atomicAdd(I.counters + 1, edges);
+            } else {
+                Isic = I.sic_val[static_cast<std::size_t>(step & 1) * I.N + c];
+            }
+            I.Isic[c] = Isic;
+        }
+
+        // Poisson drive and noise (neuron.cpp:228-248)
+        if (P.poiss_rate > 0.0) {
+            Draws r(I.seed ^ kSaltNeuronPoisson,
+                    static_cast<std::uint64_t>(step) * kStreamStride + c);
+            const int ev = r.poisson(P.lambda, P.knuth_limit);
+            if (ev > 0) exc_in += P.poiss_weight * static_cast<double>(ev);
+        }
+        double Iext = Isic;
+        if (P.noise_std > 0.0) {
+            const std::uint64_t idx = static_cast<std::uint64_t>(step / P.steps_per_noise);
+            if (P.independent_noise) {
+                Draws r(I.seed ^ kSaltNeuronNoise, idx * kNoiseStride + c);
+                Iext += 0.0 + P.noise_std * r.normal_first();
+            } else {
+                Draws r(I.seed ^ (exc ? kSaltSharedExc : kSaltSharedInh), idx);
+                Iext += 0.0 + P.noise_std * r.normal_first();
+            }
+        }
+
+        double dgex = I.dgex[c], dgin = I.dgin[c];
+        if (exc_in != 0.0) dgex += exc_in * P.psc_ex;
+        if (inh_in != 0.0) dgin += inh_in * P.psc_in;
+
+        double V = I.V[c], w = I.w[c], gex = I.gex[c], gin = I.gin[c];
+        int refr = I.refr[c];
+        const double Vr = I.V_reset[c];
+        const double h = I.ak.h;  // h_step is shared by both models
+        const double half_h = I.ak.half_h, h6 = I.ak.h6;
+        bool spiked = false;
+        for (int s = 0; s < I.ak.substeps; ++s) {
+            const double gex1 = P.decay_ex * (gex + h * dgex);
+            const double dgex1 = P.decay_ex * dgex;
+            const double gin1 = P.decay_in * (gin + h * dgin);
+            const double dgin1 = P.decay_in * dgin;
+            if (refr > 0) {
+                V = Vr;
+                const AdexRates r = adex<false>(P, V, w, gex, gin, Iext);
+                w += h * r.w;
+            } else {
+                const double gexm = 0.5 * (gex + gex1), ginm = 0.5 * (gin + gin1);
+                const AdexRates k1 = adex<true>(P, V, w, gex, gin, Iext);
+                const AdexRates k2 =
+                    adex<true>(P, V + half_h * k1.V, w + half_h * k1.w, gexm, ginm, Iext);
+                const AdexRates k3 =
+                    adex<true>(P, V + half_h * k2.V, w + half_h * k2.w, gexm, ginm, Iext);
+                const AdexRates k4 = adex<true>(P, V + h * k3.V, w + h * k3.w, gex1, gin1, Iext);
+                V += h6 * (k1.V + 2.0 * k2.V + 2.0 * k3.V + k4.V);
+                w += h6 * (k1.w + 2.0 * k2.w + 2.0 * k3.w + k4.w);
+            }
+            gex = gex1;
+            dgex = dgex1;
+            gin = gin1;
+            dgin = dgin1;
+            if (refr > 0) {
+                --refr;
+            } else if (V >= P.V_peak) {
+                V = Vr;
+                w += I.b[c];
+                refr = P.ref_steps;
+                spiked = true;
+            }
+        }
+        I.V[c] = V;
+        I.w[c] = w;
+        I.gex[c] = gex;
+        I.dgex[c] = dgex;
+        I.gin[c] = gin;
+        I.dgin[c] = dgin;
+        I.refr[c] = refr;
+
+        if (spiked) {
+            // Tsodyks-Markram update of this source (network.cpp:230-247)
+            if (I.stp_on) {
+                const double t_now = static_cast<double>(step) * I.dt;
+                const double d = t_now - I.stp_t[c];
+                const double xd = exp(-d / I.tau_rec);
+                const double ud = I.tau_fac < 1e-10 ? 0.0 : exp(-d / I.tau_fac);
+                double x = I.stp_x[c], u = I.stp_u[c];
+                x = 1.0 + (x - x * u - 1.0) * xd;
+                u = I.U + u * (1.0 - I.U) * ud;
+                I.stp_x[c] = x;
+                I.stp_u[c] = u;
+                I.stp_t[c] = t_now;
+                const std::size_t sn = static_cast<std::size_t>(slot) * I.N + c;
+                I.snap_x[sn] = x;
+                I.snap_u[sn] = u;
+            }
+            const int pos = atomicAdd(&s_nspk, 1);
+            s_spk[pos] = c;
+            if (I.rec_spikes && step >= I.rec_from) {
+                const unsigned long long li = atomicAdd(I.spike_log_n, 1ULL);
+                if (li < I.spike_log_cap) {
+                    I.spike_log[li] = (static_cast<unsigned long long>(step) << 32) | c;
+                } else {
+                    atomicAdd(I.counters + 3, 1ULL);
+                }
+            }
+            unsigned long long edges =
+                exc ? (I.exc_rs[c + 1] - I.exc_rs[c]) + (I.n2a_rs[c + 1] - I.n2a_rs[c])
+                    : (I.inh_rs[c - I.NE + 1] - I.inh_rs[c - I.NE]);
+            atomicAdd(I.counters + 0, edges);
+            atomicAdd(I.counters + 2, 1ULL);
+        }
+
+        if (I.rec_neuron_max > 0 && c < I.rec_neuron_max && step >= I.rec_from &&
+            (step - I.rec_from) % I.rec_every == 0) {
+            const std::size_t row =
+                static_cast<std::size_t>(((step - I.rec_from) / I.rec_every) % I.rec_rows);
+            I.rec_V[row * I.rec_neuron_max + c] = V;
+            I.rec_Isic[row * I.rec_neuron_max + c] = Isic;
+        }
+    }
+
+    // Push the out-edges of this block's spiking sources into the rings of
+    // their arrival steps (deliver_spikes, network.cpp:249-279).
+    __syncthreads();
+    const int nspk = s_nspk;
+    for (int q = 0; q < nspk; ++q) {
+        const std::uint32_t j = s_spk[q];
+        if (j < I.NE) {
+            const int as = static_cast<int>((step + I.d_e) % I.slots);
+            push_row(I.exc_rs, I.exc_tg, I.ring_ex, j, as);
+            push_row(I.n2a_rs, I.n2a_tg, I.ring_as, j, as);
+        } else {
+            const int as = static_cast<int>((step + I.d_i) % I.slots);
+            push_row(I.inh_rs, I.inh_tg, I.ring_in, j - I.NE, as);
+        }
+    }
+}
+
+__device__ void astro_role(const InstDev& I, const Work& wk, std::int64_t step) {
+    if (threadIdx.x >= wk.count) return;
+    const std::uint32_t a = wk.first + threadIdx.x;
+    const int slot = static_cast<int>(step % I.slots);
+    double ip3_in = 0.0;
+    {
+        const double v = ring_sum<false>(I, I.ring_as, slot, a, step - I.d_e, I.w_n2a);
+        if (v != 0.0) ip3_in += v;
+    }
+    // drive_astrocytes (network.cpp:340-355)
+    if (I.a_rate > 0.0) {
+        Draws r(I.seed ^ kSaltAstroPoisson, static_cast<std::uint64_t>(step) * kStreamStride + a);
+        const int ev = r.poisson(I.a_lambda, I.a_limit);
+        if (ev > 0) ip3_in += I.a_weight * static_cast<double>(ev);
+    }
+    // AstrocytePopulation::update (astrocyte.cpp:307-329)
+    double noise = 0.0;
+    if (I.a_std > 0.0) {
+        const std::uint64_t idx = static_cast<std::uint64_t>(step / I.a_steps_per_noise);
+        const std::uint64_t nseed = I.seed ^ kSaltAstroNoise;
+        noise = I.a_indep ? I.a_std * normal_clamped(nseed, idx * kStreamStride + a)
+                          : I.a_std * normal_clamped(nseed, idx);
+    }
+    double ca = I.Ca[a], ip3 = I.IP3[a], hh = I.h[a];
+    if (I.astro_uniform) {
+        astro_rk4(I.ak, I.Ca_tot_u, I.IP3_0_u, I.tau_u, I.delta_u, ip3_in, noise, ca, ip3, hh);
+    } else {
+        astro_rk4(I.ak, I.Ca_tot[a], I.IP3_0[a], I.tau[a], I.delta[a], ip3_in, noise, ca, ip3,
+                  hh);
+    }
+    I.Ca[a] = ca;
+    I.IP3[a] = ip3;
+    I.h[a] = hh;
+    // SIC factor of this step (astrocyte.cpp:331-339), read by the SIC sums
+    // of the arrival step.
+    if (step % I.sic_interval == 0) {
+        const double y = (ca - I.SIC_th) * 1000.0;
+        I.fac[static_cast<std::size_t>(slot) * I.NA + a] = y <= 1.0 ? 0.0 : I.SIC_scale * log(y);
+    }
+    if (I.rec_astro_max > 0 && a < I.rec_astro_max && step >= I.rec_from &&
+        (step - I.rec_from) % I.rec_every == 0) {
+        const std::size_t row =
+            static_cast<std::size_t>(((step - I.rec_from) / I.rec_every) % I.rec_rows);
+        I.rec_Ca[row * I.rec_astro_max + a] = ca;
+        I.rec_IP3[row * I.rec_astro_max + a] = ip3;
+    }
+}
+
+// SIC current arriving at step+1 (valid when d_a2n >= 2: its factors were
+// written by a launch that has completed).
+__device__ void sic_role(const InstDev& I, const Work& wk, std::int64_t step) {
+    const std::uint32_t t = wk.first + threadIdx.x;
+    const std::int64_t arr = step + 1;
+    const std::int64_t se = arr - I.d_a2n;
+    unsigned long long edges = 0;
+    // Computed even when step+1 lies past this chunk: the next chunk reads it.
+    if (threadIdx.x < wk.count && se >= 0 && se % I.sic_interval == 0) {
+        I.sic_val[static_cast<std::size_t>(arr & 1) * I.N + t] =
+            sic_sum(I, t, static_cast<int>(se % I.slots), edges);
+    }
+    // one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) edges += __shfl_down_sync(0xFFFFFFFFu, edges, o);
+    if ((threadIdx.x & 31) == 0 && edges) atomicAdd(I.counters + 1, edges);
+}
+
+__global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restrict__ insts,
+                                                         const Work* __restrict__ work, int k) {
+    // Stage this block's instance descriptor in shared memory.
+    __shared__ __align__(16) unsigned char s_raw[sizeof(InstDev)];
+    const Work wk = work[blockIdx.x];
+    {
+        const auto* src = reinterpret_cast<const std::uint32_t*>(insts + wk.inst);
+        auto* dst = reinterpret_cast<std::uint32_t*>(s_raw);
+        for (unsigned i = threadIdx.x; i < sizeof(InstDev) / 4; i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
+    const std::int64_t step = I.step0 + k;
+    if (step >= I.end_step) return;
+    if (wk.role == kRoleNeuron) {
+        neuron_role(I, wk, step);
+    } else if (wk.role == kRoleAstro) {
+        astro_role(I, wk, step);
+    } else {
+        sic_role(I, wk, step);
+    }
+}
+
+}  // namespace
+
+void launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
+                 cudaStream_t stream) {
+    step_kernel<<<n_work, block, 0, stream>>>(insts, work, k);
+}
+
+}  // namespace asg

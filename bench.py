@@ -176,7 +176,10 @@ def bench_astro_scaling(args, rank, world, pg):
     per_launch_us = dev_ms * 1e3 / args.steps
     value = n * world * args.steps / (dev_ms * 1e-3)
 
-    # e2e through the drop-in ABI: H2D input + update + D2H Ca per step.
+    # e2e through the drop-in ABI (per-cell parameter arrays, as the
+    # reference backend holds them): H2D input + update + D2H Ca per step.
+    eng_e2e = AstroBackend(Ca, IP3, h, np.full(n, w.Ca_tot), np.full(n, w.IP3_0),
+                           np.full(n, w.tau_IP3), np.full(n, w.delta_IP3))
     ein_t, ein = pinned(n)
     eca_t, eca = pinned(n)
     rng_inputs = []
@@ -188,9 +191,9 @@ def bench_astro_scaling(args, rank, world, pg):
     e2e_steps = max(3, min(args.steps, 20))
     for k in range(2):  # warm-up of the copy path
         ein[:] = rng_inputs[k % 2]
-        eng.push_input(ein)
-        eng.update(w.consts, w.h_step, w.substeps)
-        eca[:] = eng.pull_calcium()
+        eng_e2e.push_input(ein)
+        eng_e2e.update(w.consts, w.h_step, w.substeps)
+        eca[:] = eng_e2e.pull_calcium()
     torch.cuda.synchronize()
     barrier(pg)
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -198,15 +201,14 @@ def bench_astro_scaling(args, rank, world, pg):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ev0.record()
-    lib = eng  # noqa: F841
     from astrosimgpu_b200 import _lib
     L = _lib.load()
     for k in range(e2e_steps):
         ein[:] = rng_inputs[k % 2]
-        _lib.check(L.asg_astro_push_input(eng._h, _lib.dptr(ein)), "push")
-        _lib.check(L.asg_astro_update(eng._h, _lib.dptr(w.consts), w.h_step, w.substeps, 0.0, 1,
-                                      0.0, 0, 0), "update")
-        _lib.check(L.asg_astro_pull_calcium(eng._h, _lib.dptr(eca)), "pull")
+        _lib.check(L.asg_astro_push_input(eng_e2e._h, _lib.dptr(ein)), "push")
+        _lib.check(L.asg_astro_update(eng_e2e._h, _lib.dptr(w.consts), w.h_step, w.substeps, 0.0,
+                                      1, 0.0, 0, 0), "update")
+        _lib.check(L.asg_astro_pull_calcium(eng_e2e._h, _lib.dptr(eca)), "pull")
     ev1.record()
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
@@ -214,6 +216,7 @@ def bench_astro_scaling(args, rank, world, pg):
     wall = max_over_ranks(pg, wall)
     e2e_value = n * world * e2e_steps / wall
     del ein_t, eca_t
+    eng_e2e.destroy()
 
     peak, peak_kind = load_peaks()
     achieved = BYTES_PER_CELL_STEP * n / (per_launch_us * 1e-6) / 1e9
@@ -231,6 +234,29 @@ def bench_astro_scaling(args, rank, world, pg):
         "clocks": clk.summary(),
     }
     return out, (w, Ca, IP3, h)
+
+
+def bench_network(name="paper_sparse_dt005", warm=200, steps=2000, **opts):
+    """Plain one-network path on a shipped config: device time per step."""
+    from astrosimgpu_b200 import _lib
+    from astrosimgpu_b200.network import Model, Network, config_path
+    t0 = time.perf_counter()
+    m = Model(config_path(name), pre_time=0.0)
+    build_s = time.perf_counter() - t0
+    net = Network(m, record=_lib.RecordOpts(0, 10, 1, 0, 0), **opts)
+    net.step(warm)
+    c0 = net.counters()
+    net.step(steps)
+    ms, kernels = net.last_timing()
+    c1 = net.counters()
+    n = net.n
+    events = (c1["spike_edges"] - c0["spike_edges"]) + (c1["sic_edges"] - c0["sic_edges"])
+    us = ms * 1e3 / steps
+    return {"config": name, "neurons": n, "astrocytes": net.na, "dt_ms": m.dt,
+            "us_per_step": us, "neuron_updates_per_s": n / (us * 1e-6),
+            "synaptic_events_per_s": events / (ms * 1e-3),
+            "sim_s_per_wall_s": (m.dt * 1e-3) / (us * 1e-6), "kernels": kernels,
+            "spikes": c1["spikes"] - c0["spikes"], "build_s": build_s, "steps": steps}
 
 
 def reference_cuda_kernel(w, Ca, IP3, h, steps):
@@ -346,6 +372,10 @@ def main():
                                                                     min(args.steps, 50))
         except Exception as e:  # noqa: BLE001
             extras["reference_cuda_kernel"] = {"unavailable": str(e)[:200]}
+        try:
+            extras["network_c2"] = bench_network()
+        except Exception as e:  # noqa: BLE001
+            extras["network_c2"] = {"unavailable": str(e)[:300]}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w)

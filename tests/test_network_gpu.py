@@ -1,0 +1,215 @@
+"""The whole per-timestep path on the B200 against the reference simulator
+built from its own sources (oracle/_ref), on the same config and seed.
+
+Parity bar (stated tolerances):
+- spike rasters identical over the horizon run here;
+- state within 1e-12 relative (|a-b| <= 1e-12 * max(|b|, 1e-3)) over the
+  same horizon.  Arithmetic is evaluated in the reference's order without
+  contraction; the only source of difference is the last bit of CUDA's
+  exp/log/cos against the host libm on data-dependent arguments.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from astrosimgpu_b200 import _lib
+from astrosimgpu_b200.network import Batch, Model, Network, config_path
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+STATE_KEYS = ("V", "w", "g_ex", "dg_ex", "g_in", "dg_in", "I_sic", "Ca", "IP3", "h")
+
+
+def rec_all():
+    return _lib.RecordOpts(0, 10, 1, 0, 0)
+
+
+def run_pair(path=None, text=None, steps=1000, chunks=1, **opts):
+    m = Model(path=path, text=text, pre_time=0.0)
+    g = Network(m, record=rec_all(), **opts)
+    r = ref.RefNetwork(path=path, text=text, pre_time=0.0)
+    per = steps // chunks
+    for _ in range(chunks):
+        g.step(per)
+    gs, gsrc = g.fetch_spikes()
+    rs, rsrc = r.run(per * chunks)
+    return g, r, (gs, gsrc), (rs, rsrc)
+
+
+def assert_state_close(g, r, rel=REL):
+    a, b = g.state(), r.state()
+    worst = 0.0
+    for k in STATE_KEYS:
+        d = np.abs(a[k] - b[k]) / np.maximum(np.abs(b[k]), 1e-3)
+        worst = max(worst, float(d.max()) if d.size else 0.0)
+        assert np.all(d <= rel), (k, float(d.max()))
+    assert np.array_equal(a["refractory"], b["refractory"])
+    return worst
+
+
+def assert_same_spikes(gsp, rsp):
+    (gs, gsrc), (rs, rsrc) = gsp, rsp
+    if not (np.array_equal(gs, rs) and np.array_equal(gsrc, rsrc)):
+        n = min(len(gs), len(rs))
+        bad = np.nonzero((gs[:n] != rs[:n]) | (gsrc[:n] != rsrc[:n]))[0]
+        first = int(bad[0]) if len(bad) else n
+        raise AssertionError(f"rasters differ at spike #{first} (gpu {len(gs)} vs ref {len(rs)}) "
+                             f"step {gs[first] if first < len(gs) else None}")
+
+
+@pytest.mark.parametrize("name,steps", [("quick", 4000), ("use_case", 3000), ("bursting", 3000),
+                                        ("random_pool", 2000), ("c0_literal", 1500),
+                                        ("no_spiking", 1000)])
+def test_config_parity(name, steps):
+    g, r, gsp, rsp = run_pair(config_path(name), steps=steps, chunks=2)
+    assert_same_spikes(gsp, rsp)
+    assert len(gsp[0]) > 0 or name == "no_spiking"
+    assert_state_close(g, r)
+    # STP per source equals every edge of that source
+    x, u, t = g.stp()
+    tab = r.table(0)
+    rs = tab["row_start"]
+    for s in range(0, len(rs) - 1, 7):
+        if rs[s] < rs[s + 1]:
+            e = rs[s]
+            assert x[s] == tab["stp_x"][e] and u[s] == tab["stp_u"][e]
+
+
+def test_paper_sparse_shape_parity():
+    """10k neurons, 10k astrocytes, ~10M synapses, dt 0.05 ms, 1.5 ms delays."""
+    g, r, gsp, rsp = run_pair(config_path("paper_sparse_dt005"), steps=600, chunks=3)
+    assert_same_spikes(gsp, rsp)
+    assert len(gsp[0]) > 0
+    assert_state_close(g, r)
+    c = g.counters()
+    assert c["sic_edges"] > 0 and c["spike_edges"] > 0
+
+
+def variants():
+    base = json.load(open(config_path("quick")))
+    out = []
+    v = json.loads(json.dumps(base))
+    for k in ("input_exc", "input_inh", "input_astro"):
+        v[k]["independent_noise"] = False
+    out.append(("shared_noise", v))
+    v = json.loads(json.dumps(base))
+    v["synapse"]["stp"]["enabled"] = False
+    out.append(("stp_off", v))
+    v = json.loads(json.dumps(base))
+    v["synapse"]["stp"]["tau_fac"] = 50.0
+    v["synapse"]["sic_interval"] = 7
+    v["connectivity"]["unique_third_out"] = True
+    out.append(("fac_interval_unique", v))
+    v = json.loads(json.dumps(base))
+    v["synapse"]["d_a2n"] = 0.1  # one-step SIC delay: fused SIC path
+    v["synapse"]["d_i"] = 0.3
+    v["simulation"]["substeps"] = 3
+    v["neuron_exc"]["t_ref"] = 2.0
+    out.append(("short_delays_substeps_refractory", v))
+    v = json.loads(json.dumps(base))
+    v["synapse"]["w_e"] = -2.0  # negative excitatory weight routes to the inhibitory input
+    v["synapse"]["w_i"] = 3.0
+    v["input_exc"]["poiss_rate"] = 400000.0  # lambda > 30: normal approximation
+    out.append(("sign_routing_big_lambda", v))
+    return out
+
+
+@pytest.mark.parametrize("label,cfg", variants(), ids=[v[0] for v in variants()])
+def test_variant_parity(label, cfg):
+    g, r, gsp, rsp = run_pair(text=json.dumps(cfg), steps=2000, chunks=2)
+    assert_same_spikes(gsp, rsp)
+    assert_state_close(g, r)
+
+
+def test_sic_modes_and_block_sizes_bitwise():
+    """The separate SIC role and the fused form, and any block size, give
+    identical bits (the arithmetic per cell does not depend on the launch)."""
+    path = config_path("use_case")
+    m = Model(path, pre_time=0.0)
+    outs = []
+    for opts in (dict(sic_mode=1, block_neuron=64), dict(sic_mode=2, block_neuron=256),
+                 dict(sic_mode=0, block_neuron=128, chunk_steps=7, use_graphs=-1)):
+        n = Network(m, record=rec_all(), **opts)
+        n.step(1200)
+        outs.append((n.fetch_spikes(), n.state()))
+    for (sp, st) in outs[1:]:
+        assert np.array_equal(sp[0], outs[0][0][0]) and np.array_equal(sp[1], outs[0][0][1])
+        for k in STATE_KEYS:
+            assert np.array_equal(st[k], outs[0][1][k]), k
+
+
+def test_batch_equals_single_bitwise():
+    """Instances of uneven size packed into one engine give the bits each
+    gives alone."""
+    names = ["quick", "use_case", "quick", "bursting"]
+    seeds = [1, 2, 3, 4]
+    models = [Model(config_path(n), seed=s, pre_time=0.0) for n, s in zip(names, seeds)]
+    b = Batch(models, record=rec_all())
+    b.step(800)
+    for i, m in enumerate(models):
+        n = Network(m, record=rec_all())
+        n.step(800)
+        s1, s2 = n.fetch_spikes(), b.fetch_spikes(i)
+        assert np.array_equal(s1[0], s2[0]) and np.array_equal(s1[1], s2[1])
+        a, c = n.state(), b.state(i)
+        for k in STATE_KEYS:
+            assert np.array_equal(a[k], c[k]), (i, k)
+
+
+def test_checkpoint_restore_bitwise():
+    m = Model(config_path("use_case"), pre_time=0.0)
+    n = Network(m, record=rec_all())
+    n.step(500)
+    blob = n.checkpoint()
+    n.fetch_spikes()
+    n.step(700)
+    sp1, st1 = n.fetch_spikes(), n.state()
+    n.restore(blob)
+    n.step(700)
+    sp2, st2 = n.fetch_spikes(), n.state()
+    assert np.array_equal(sp1[0], sp2[0]) and np.array_equal(sp1[1], sp2[1])
+    for k in STATE_KEYS:
+        assert np.array_equal(st1[k], st2[k]), k
+
+
+def test_recording_matches_reference_rows():
+    """Recorded Ca/IP3 rows of the first cells every record_every steps, as
+    Network::run writes them (network.cpp:443-462)."""
+    path = config_path("quick")
+    m = Model(path, pre_time=0.0)
+    n = Network(m, record=_lib.RecordOpts(0, 10, 1, 20, 15))
+    r = ref.RefNetwork(path=path, pre_time=0.0)
+    n.step(300)
+    rec = n.fetch_record()
+    assert len(rec["astro_steps"]) == 30 and rec["astro_steps"][-1] == 290
+    # replay the reference to step 291 and compare the last row
+    r.run(291)
+    s = r.state()
+    assert np.allclose(rec["Ca"][-1], s["Ca"][:20], rtol=REL, atol=0)
+    assert np.allclose(rec["IP3"][-1], s["IP3"][:20], rtol=REL, atol=0)
+
+
+def test_fixed_indegree_device_equals_host():
+    text = json.dumps({"N": {"N_A": 5000, "N_E": 4000, "N_I": 1000},
+                       "connectivity": {"p_third_if_primary": 0.7, "pool_size": 3,
+                                        "pool_type": "random"}})
+    h = Model(text=text, fixed_indegree=50)
+    d = Model(text=text, fixed_indegree=50, gen_device=0)
+    for which in range(4):
+        a, b = h.table(which), d.table(which)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), which
+
+
+def test_bad_descriptor_is_rejected_cleanly():
+    m = Model(config_path("quick"), pre_time=0.0)
+    d = m.desc()
+    bad = _lib.NetworkDesc.from_buffer_copy(d)
+    bad.d_e_steps = 0
+    import ctypes as C
+    h = C.c_void_p()
+    st = _lib.load().asg_create(C.byref(bad), None, None, C.byref(h))
+    assert st == 1 and not h
+    assert b"delay" in _lib.load().asg_last_error()
