@@ -221,6 +221,7 @@ Engine::~Engine() {
         if (h_insts[p]) cudaFreeHost(h_insts[p]);
         if (h_stats[p]) cudaFreeHost(h_stats[p]);
         if (ev_chunk[p]) cudaEventDestroy(ev_chunk[p]);
+        if (ev_chunk0[p]) cudaEventDestroy(ev_chunk0[p]);
     }
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_end) cudaEventDestroy(ev_end);
@@ -248,7 +249,10 @@ int Engine::init() {
     ASG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     ASG_CUDA(cudaEventCreate(&ev_start));
     ASG_CUDA(cudaEventCreate(&ev_end));
-    for (int p = 0; p < 2; ++p) ASG_CUDA(cudaEventCreateWithFlags(&ev_chunk[p], cudaEventDisableTiming));
+    for (int p = 0; p < 2; ++p) {
+        ASG_CUDA(cudaEventCreate(&ev_chunk[p]));
+        ASG_CUDA(cudaEventCreate(&ev_chunk0[p]));
+    }
     return ASG_OK;
 }
 
@@ -451,6 +455,9 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     ring_segs(D.ring_ex, rex, N);
     ring_segs(D.ring_in, rin, N);
     ring_segs(D.ring_as, ras, NA);
+    D.ring_ex.src_base = 0;
+    D.ring_in.src_base = NE;  // inhibitory rows are numbered from the first inhibitory cell
+    D.ring_as.src_base = 0;
     add_seg(D.sic_soff, sic.soff.size() * 4, sic.soff.data());
     add_seg(D.sic_ent, sic.ent.size() * 4, sic.ent.data());
     add_seg(D.fac, S * std::max<std::size_t>(a8, 8), nullptr);
@@ -499,6 +506,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
         std::max<std::uint64_t>(1, std::min<std::uint64_t>(full, std::max<std::uint64_t>(
                                                                      65536, full / 8))));
     I.keep_spikes = keep_spikes;
+    I.max_chunk = cfg.chunk_steps;
     const std::size_t rec_doubles =
         static_cast<std::size_t>(I.rec_rows) * (2 * D.rec_astro_max + 2 * D.rec_neuron_max) + 1;
     for (int p = 0; p < 2; ++p) {
@@ -545,12 +553,12 @@ int Engine::set_block(int block) {
 
 int Engine::set_chunk(int chunk) {
     if (chunk < 1) return fail(ASG_ERR_ARG, "chunk must be >= 1");
-    // Record rings are sized by the chunk at add(); keep chunks within them.
+    // Output buffers were sized for the chunk in force when each instance
+    // was added; a longer chunk could overrun them.
     for (auto& p : insts)
-        if (static_cast<std::uint32_t>(chunk / p->dev.rec_every + 2) > p->rec_rows ||
-            static_cast<std::uint64_t>(chunk) * p->dev.N > 8ull * p->log_cap + 65536ull * 8)
-            return fail(ASG_ERR_ARG, "chunk %d exceeds the output buffers sized at creation",
-                        chunk);
+        if (chunk > p->max_chunk)
+            return fail(ASG_ERR_ARG, "chunk %d exceeds %d, the chunk instance %d was sized for",
+                        chunk, p->max_chunk, p->id);
     cfg.chunk_steps = chunk;
     dirty = true;
     return ASG_OK;
@@ -643,6 +651,7 @@ int Engine::launch_chunk(int parity, int steps) {
         I.chunk_first[parity] = I.step;
         I.chunk_last[parity] = D.end_step;
     }
+    ASG_CUDA(cudaEventRecord(ev_chunk0[parity], stream));
     ASG_CUDA(cudaMemcpyAsync(d_insts.get(), hi, insts.size() * sizeof(InstDev),
                              cudaMemcpyHostToDevice, stream));
     if (graph != nullptr && steps == graph_steps) {
@@ -654,6 +663,7 @@ int Engine::launch_chunk(int parity, int steps) {
         ASG_CUDA(cudaGetLastError());
     }
     last_kernels += steps;
+    launched_kernels += steps;
     ASG_CUDA(cudaMemcpyAsync(h_stats[parity], d_stats.get(),
                              insts.size() * 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              stream));
@@ -669,6 +679,9 @@ int Engine::collect(int parity) {
     if (!pending[parity]) return ASG_OK;
     ASG_CUDA(cudaEventSynchronize(ev_chunk[parity]));
     pending[parity] = false;
+    float chunk_ms = 0.0f;
+    if (cudaEventElapsedTime(&chunk_ms, ev_chunk0[parity], ev_chunk[parity]) == cudaSuccess)
+        chunk_device_ms += chunk_ms;
     const unsigned long long* st = h_stats[parity];
     for (std::size_t s = 0; s < insts.size(); ++s) {
         Instance& I = *insts[s];

@@ -66,6 +66,8 @@ struct InRing {
     std::uint32_t* cnt;           // [slots][n_targets] set bits pending per target
     std::uint32_t words;          // total bitmap words of one slot
     std::uint32_t n_targets;
+    std::uint32_t src_base;       // global neuron index of local source 0
+    std::uint32_t pad;
 };
 
 struct InstDev {

@@ -47,6 +47,7 @@ struct Instance {
     std::int64_t chunk_first[2] = {0, 0};   // first step of the chunk written to parity p
     std::int64_t chunk_last[2] = {0, 0};
     bool keep_spikes = true;
+    int max_chunk = 0;  // longest chunk the output buffers were sized for
     ~Instance();
 };
 
@@ -79,6 +80,9 @@ public:
     // One chunk of up to chunk_steps (serving loop granularity).
     int run_chunk(std::int64_t max_steps);
 
+    // Waits for every chunk in flight and gathers its outputs.
+    int flush() { return finish_pending(); }
+
     int pull_state(int id, asg_state* out);
     int pull_stp(int id, double* x, double* u, double* t);
 
@@ -89,6 +93,8 @@ public:
     double total_ms = 0.0;
     std::int64_t total_kernels = 0;
     std::int64_t chunks = 0;
+    double chunk_device_ms = 0.0;  // sum over collected chunks (serving)
+    std::int64_t launched_kernels = 0;
     std::uint64_t resident_bytes = 0;
     cudaStream_t stream = nullptr;
     int sms = 148;
@@ -114,6 +120,7 @@ private:
     bool dirty = true;
     cudaEvent_t ev_start = nullptr, ev_end = nullptr;
     cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
+    cudaEvent_t ev_chunk0[2] = {nullptr, nullptr};
     bool pending[2] = {false, false};
     int next_parity = 0;
     int next_id = 0;

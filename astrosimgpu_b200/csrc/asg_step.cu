@@ -47,7 +47,7 @@ __device__ __forceinline__ double ring_sum(const InstDev& I, const InRing& R, in
         while (word != 0) {
             const int b = __ffs(word) - 1;
             word &= word - 1;
-            const std::uint32_t j = src[(q - w0) * 32 + b];
+            const std::uint32_t j = R.src_base + src[(q - w0) * 32 + b];
             const double c = I.stp_on ? weight * I.snap_x[snap + j] * I.snap_u[snap + j] : weight;
             if (kSubtract) {
                 acc -= c;

@@ -259,6 +259,80 @@ def bench_network(name="paper_sparse_dt005", warm=200, steps=2000, **opts):
             "spikes": c1["spikes"] - c0["spikes"], "build_s": build_s, "steps": steps}
 
 
+def bench_batched(sim_ms=500.0, n_inst=64, autotune=True):
+    """64-instance sweep: batched engine vs one network per launch."""
+    from astrosimgpu_b200 import _lib
+    from astrosimgpu_b200.network import Batch, Model, Network
+    from astrosimgpu_b200.workloads import sweep_configs
+    texts = sweep_configs(n_inst, sim_ms)
+    models = [Model(text=t, pre_time=0.0) for t in texts]
+    steps = models[0].sim_steps
+    dt = models[0].dt
+    rec = _lib.RecordOpts(0, 10, 1, 0, 0)
+    # plain path: each instance on its own, one after another
+    plain_ms, plain_kernels = 0.0, 0
+    for m in models:
+        net = Network(m, record=rec, chunk_steps=64)
+        net.step(64)  # warm (graph capture)
+        net.step(steps)
+        ms, k = net.last_timing()
+        plain_ms += ms
+        plain_kernels += k
+        net.close()
+    b = Batch(models, record=rec, chunk_steps=128)
+    tuned = b.autotune(256) if autotune else None
+    b.step(64)
+    b.step(steps)
+    bms, bk = b.last_timing()
+    sim_s = n_inst * steps * dt * 1e-3
+    spikes = sum(b.counters(i)["spikes"] for i in range(n_inst))
+    neurons = sum(mm.desc().n_exc + mm.desc().n_inh for mm in models)
+    return {"instances": n_inst, "steps": steps, "sim_ms_each": steps * dt,
+            "total_neurons": neurons,
+            "batched_ms": bms, "plain_ms": plain_ms,
+            "batched_sim_s_per_wall_s": sim_s / (bms * 1e-3),
+            "plain_sim_s_per_wall_s": sim_s / (plain_ms * 1e-3),
+            "speedup": plain_ms / bms, "batched_kernels": bk, "plain_kernels": plain_kernels,
+            "batched_us_per_step": bms * 1e3 / steps, "autotuned": tuned,
+            "spikes": spikes}
+
+
+def bench_serving(n_req=30, rate_hz=20.0, big=False, **opts):
+    """Poisson request stream through the continuous-batching server."""
+    import numpy as np
+    from astrosimgpu_b200.network import Model, Server
+    from astrosimgpu_b200.workloads import request_stream, serving_config
+    stream = request_stream(n_req, rate_hz, big=big)
+    t0 = time.perf_counter()
+    models = [Model(text=serving_config(n, sd, dur), pre_time=0.0, fixed_indegree=100,
+                    gen_device=0) for (_, n, dur, sd) in stream]
+    build_s = time.perf_counter() - t0
+    srv = Server(**opts)
+    ids = []
+    start = time.perf_counter()
+    for (arr, n, dur, sd), m in zip(stream, models):
+        delay = arr - (time.perf_counter() - start)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(m, m.sim_steps, keep_spikes=False))
+    res = [srv.wait(i) for i in ids]
+    wall = time.perf_counter() - start
+    st = srv.stats()
+    srv.close()
+    lat = np.array([r.submit_to_done_ms for r in res])
+    events = sum(r.spike_edges + r.sic_edges for r in res)
+    sim_s = sum(dur for (_, _, dur, _) in stream) * 1e-3
+    neuron_steps = sum(n * m.sim_steps for (_, n, _, _), m in zip(stream, models))
+    return {"requests": len(res), "arrival_rate_hz": rate_hz,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "wall_s": wall, "synaptic_events_per_s": events / wall,
+            "sim_s_per_wall_s": sim_s / wall, "neuron_updates_per_s": neuron_steps / wall,
+            "peak_resident": st["peak_resident"], "kernels": st["kernels"],
+            "device_ms": st["device_ms"], "build_s": build_s,
+            "sizes": [int(n) for (_, n, _, _) in stream],
+            "statuses": sorted(set(int(r.status) for r in res))}
+
+
 def reference_cuda_kernel(w, Ca, IP3, h, steps):
     """The reference's astro_update_kernel (sm_100a build) on the same GPU."""
     import numpy as np
@@ -350,6 +424,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the reference CUDA kernel and sub-benchmarks")
+    ap.add_argument("--skip", default="", help="comma list of sub-benchmarks to skip: "
+                    "network_c2,batched_c3,serving_c4")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -372,10 +448,14 @@ def main():
                                                                     min(args.steps, 50))
         except Exception as e:  # noqa: BLE001
             extras["reference_cuda_kernel"] = {"unavailable": str(e)[:200]}
-        try:
-            extras["network_c2"] = bench_network()
-        except Exception as e:  # noqa: BLE001
-            extras["network_c2"] = {"unavailable": str(e)[:300]}
+        for key, fn in (("network_c2", bench_network), ("batched_c3", bench_batched),
+                        ("serving_c4", bench_serving)):
+            if key in args.skip:
+                continue
+            try:
+                extras[key] = fn()
+            except Exception as e:  # noqa: BLE001
+                extras[key] = {"unavailable": f"{type(e).__name__}: {str(e)[:300]}"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w)
