@@ -286,6 +286,9 @@ int Engine::footprint(const asg_network_desc& d, int chunk_steps, std::uint64_t*
 
 int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int64_t first,
                 std::int64_t end, bool keep_spikes, int* id_out) {
+    // Chunks in flight report statistics by instance position: gather them
+    // before the instance list changes.
+    ASG_TRY(finish_pending());
     const std::uint32_t NE = d.n_exc, NI = d.n_inh, N = NE + NI, NA = d.n_astro;
     if (d.dt <= 0.0) return fail(ASG_ERR_ARG, "dt must be positive");
     if (d.substeps < 1) return fail(ASG_ERR_ARG, "substeps must be at least 1");
@@ -671,6 +674,7 @@ int Engine::launch_chunk(int parity, int steps) {
                              stream));
     ASG_CUDA(cudaEventRecord(ev_chunk[parity], stream));
     pending[parity] = true;
+    launched_insts[parity] = insts.size();
     for (auto& p : insts) p->step = std::min<std::int64_t>(p->end, p->step + steps);
     return ASG_OK;
 }
@@ -683,7 +687,8 @@ int Engine::collect(int parity) {
     if (cudaEventElapsedTime(&chunk_ms, ev_chunk0[parity], ev_chunk[parity]) == cudaSuccess)
         chunk_device_ms += chunk_ms;
     const unsigned long long* st = h_stats[parity];
-    for (std::size_t s = 0; s < insts.size(); ++s) {
+    const std::size_t n_launched = std::min(insts.size(), launched_insts[parity]);
+    for (std::size_t s = 0; s < n_launched; ++s) {
         Instance& I = *insts[s];
         const InstDev& D = I.dev;
         const unsigned long long* c = st + s * 8;

@@ -122,6 +122,7 @@ private:
     cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
     cudaEvent_t ev_chunk0[2] = {nullptr, nullptr};
     bool pending[2] = {false, false};
+    std::size_t launched_insts[2] = {0, 0};
     int next_parity = 0;
     int next_id = 0;
 };

@@ -168,7 +168,10 @@ void Server::loop() {
             }
             if (resident >= max_instances || resident_bytes + r.footprint > budget) break;
             int id = -1;
-            const int st = eng->add(r.desc->d, nullptr, 0, r.n_steps, r.keep_spikes, &id);
+            asg_record_opts ro{};
+            ro.record_every = 1;
+            ro.spikes = r.keep_spikes ? 1 : 0;
+            const int st = eng->add(r.desc->d, &ro, 0, r.n_steps, r.keep_spikes, &id);
             if (st == ASG_ERR_OOM && resident > 0) break;  // wait for memory to free up
             queue.pop_front();
             if (st != ASG_OK) {

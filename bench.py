@@ -426,6 +426,9 @@ def main():
                     help="skip the reference CUDA kernel and sub-benchmarks")
     ap.add_argument("--skip", default="", help="comma list of sub-benchmarks to skip: "
                     "network_c2,batched_c3,serving_c4")
+    ap.add_argument("--only", default="", choices=["", "astro", "network_c2", "batched_c3",
+                                                   "serving_c4"],
+                    help="run one part alone and print its JSON (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -439,7 +442,15 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.only and args.only != "astro":
+        fn = {"network_c2": lambda: bench_network(warm=args.warmup, steps=args.steps),
+              "batched_c3": bench_batched, "serving_c4": bench_serving}[args.only]
+        print(json.dumps({args.only: fn()}), flush=True)
+        return 0
     res, (w, Ca, IP3, h) = bench_astro_scaling(args, rank, world, pg)
+    if args.only == "astro":
+        print(json.dumps({"astro": {k: res[k] for k in ("value", "per_launch_us", "roofline")}}))
+        return 0
 
     extras = {}
     if rank == 0 and not args.no_extras:

@@ -84,8 +84,7 @@ def test_paper_sparse_shape_parity():
     assert_same_spikes(gsp, rsp)
     assert len(gsp[0]) > 0
     assert_state_close(g, r)
-    c = g.counters()
-    assert c["sic_edges"] > 0 and c["spike_edges"] > 0
+    assert g.counters()["spike_edges"] > 0
 
 
 def variants():
@@ -114,6 +113,13 @@ def variants():
     v["synapse"]["w_i"] = 3.0
     v["input_exc"]["poiss_rate"] = 400000.0  # lambda > 30: normal approximation
     out.append(("sign_routing_big_lambda", v))
+    v = json.loads(json.dumps(base))
+    # astrocytes above the SIC threshold from the start, random pools of 5:
+    # SIC sums over several astrocytes with multiplicities from step d_a2n on
+    v["astrocyte"]["Ca_init"] = 0.35
+    v["astrocyte"]["IP3"] = 0.6
+    v["connectivity"].update({"pool_type": "random", "pool_size": 5, "p_third_if_primary": 0.6})
+    out.append(("active_astrocytes_random_pools", v))
     return out
 
 
@@ -122,6 +128,8 @@ def test_variant_parity(label, cfg):
     g, r, gsp, rsp = run_pair(text=json.dumps(cfg), steps=2000, chunks=2)
     assert_same_spikes(gsp, rsp)
     assert_state_close(g, r)
+    if label == "active_astrocytes_random_pools":
+        assert g.counters()["sic_edges"] > 0
 
 
 def test_sic_modes_and_block_sizes_bitwise():
