@@ -68,9 +68,12 @@ AstroK make_astro_k(const asg_astro_params& a, double h, int substeps) {
     return k;
 }
 
-// Transposed in-edge structure of one set (host arrays).
+// Transposed in-edge structure of one set (host arrays).  A target's
+// in-edges are numbered p = 0.. in (source, row position) order; bit p of the
+// target's words marks an arrival on that edge.
 struct InRingHost {
-    std::vector<std::uint32_t> row, src, wbase, bitpos;
+    std::vector<std::uint32_t> wbase, bitpos;
+    std::vector<std::uint8_t> sbit;
     std::uint32_t words = 0;
 };
 
@@ -78,26 +81,24 @@ InRingHost make_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std:
                         std::uint32_t n_targets) {
     InRingHost r;
     const std::uint32_t m = rs[n_src];
-    r.row.assign(n_targets + 1, 0);
-    for (std::uint32_t e = 0; e < m; ++e) r.row[tg[e] + 1]++;
-    for (std::uint32_t t = 0; t < n_targets; ++t) r.row[t + 1] += r.row[t];
+    std::vector<std::uint32_t> deg(n_targets, 0);
+    for (std::uint32_t e = 0; e < m; ++e) deg[tg[e]]++;
     r.wbase.assign(n_targets + 1, 0);
-    for (std::uint32_t t = 0; t < n_targets; ++t) {
-        const std::uint32_t deg = r.row[t + 1] - r.row[t];
-        r.wbase[t + 1] = r.wbase[t] + (deg + 31) / 32;
-    }
+    for (std::uint32_t t = 0; t < n_targets; ++t) r.wbase[t + 1] = r.wbase[t] + (deg[t] + 31) / 32;
     r.words = r.wbase[n_targets];
-    r.src.assign(m, 0);
     r.bitpos.assign(m, 0);
-    std::vector<std::uint32_t> fill(r.row.begin(), r.row.end() - 1);
-    // Sources ascending, each row in CSR order: every in-list comes out
-    // sorted by (source, position in the source's row).
+    r.sbit.assign(m, 0);
+    std::vector<std::uint32_t> next(n_targets, 0);
+    // Sources ascending, each row in CSR order: in-edge numbers follow
+    // (source, position in the source's row).
     for (std::uint32_t s = 0; s < n_src; ++s) {
         for (std::uint32_t e = rs[s]; e < rs[s + 1]; ++e) {
             const std::uint32_t t = tg[e];
-            const std::uint32_t p = fill[t]++;
-            r.src[p] = s;
-            r.bitpos[e] = r.wbase[t] * 32 + (p - r.row[t]);
+            const std::uint32_t p = next[t]++;
+            const std::uint32_t nw = r.wbase[t + 1] - r.wbase[t];
+            const std::uint32_t G = (nw + 63) / 64;
+            r.bitpos[e] = r.wbase[t] * 32 + p;
+            r.sbit[e] = static_cast<std::uint8_t>((p / 32) / G);
         }
     }
     return r;
@@ -274,9 +275,9 @@ int Engine::footprint(const asg_network_desc& d, int chunk_steps, std::uint64_t*
                         Ea = edges(d.neuron_astro), Es = edges(d.astro_neuron);
     std::uint64_t b = 0;
     b += N * (7 * 8 + 4 + 16 + 24) + NA * (7 * 8);  // state, params, STP
-    b += slots * N * 16;                              // snapshots
-    b += (Ee + Ei + Ea) * 16 + (N * 3 + NA) * 12;     // out/in lists + row arrays
-    b += slots * ((Ee + Ei + Ea) / 32 + 2 * N + NA) * 4 + slots * (2 * N + NA) * 4;  // bits+cnt
+    const std::uint64_t words = (Ee + Ei + Ea) / 32 + 2 * N + NA;  // upper bound
+    b += (Ee + Ei + Ea) * 9 + (N * 3 + NA) * 8;       // out lists, bit positions, word bases
+    b += slots * words * (4 + 32 * 8) + slots * (2 * N + NA) * 8;  // bits, values, summaries
     b += Es * 4 + N * 8 + slots * NA * 8 + 2 * N * 8;  // SIC (upper bound), factors, values
     b += 256 * 64;                                     // alignment slack
     (void)chunk_steps;
@@ -437,8 +438,6 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     add_seg(D.stp_x, n8, stp_x.data());
     add_seg(D.stp_u, n8, stp_u.data());
     add_seg(D.stp_t, n8, stp_t.data());
-    add_seg(D.snap_x, S * n8, nullptr);
-    add_seg(D.snap_u, S * n8, nullptr);
     add_seg(D.exc_rs, (NE + 1) * 4, d.exc_primary.n_sources ? d.exc_primary.row_start : zero_rs);
     add_seg(D.exc_tg, e4(d.exc_primary), d.exc_primary.target);
     add_seg(D.inh_rs, (NI + 1) * 4, d.inh_primary.n_sources ? d.inh_primary.row_start : zero_rs);
@@ -446,21 +445,20 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     add_seg(D.n2a_rs, (NE + 1) * 4, d.neuron_astro.n_sources ? d.neuron_astro.row_start : zero_rs);
     add_seg(D.n2a_tg, e4(d.neuron_astro), d.neuron_astro.target);
     auto ring_segs = [&](InRing& R, InRingHost& H, std::uint32_t n_t) {
-        add_seg(R.row, H.row.size() * 4, H.row.data());
-        add_seg(R.src, H.src.size() * 4, H.src.data());
+        const std::size_t W = std::max<std::uint32_t>(H.words, 1);
         add_seg(R.wbase, H.wbase.size() * 4, H.wbase.data());
         add_seg(R.bitpos, H.bitpos.size() * 4, H.bitpos.data());
-        add_seg(R.bits, S * std::max<std::uint32_t>(H.words, 1) * 4, nullptr);
-        add_seg(R.cnt, S * std::max<std::uint32_t>(n_t, 1) * 4, nullptr);
+        add_seg(R.sbit, H.sbit.size(), H.sbit.data());
+        add_seg(R.bits, S * W * 4, nullptr);
+        add_seg(R.sum, S * std::max<std::uint32_t>(n_t, 1) * 8, nullptr);
+        add_seg(R.vals, S * W * 32 * 8, nullptr);
         R.words = H.words;
         R.n_targets = n_t;
     };
     ring_segs(D.ring_ex, rex, N);
     ring_segs(D.ring_in, rin, N);
     ring_segs(D.ring_as, ras, NA);
-    D.ring_ex.src_base = 0;
-    D.ring_in.src_base = NE;  // inhibitory rows are numbered from the first inhibitory cell
-    D.ring_as.src_base = 0;
+
     add_seg(D.sic_soff, sic.soff.size() * 4, sic.soff.data());
     add_seg(D.sic_ent, sic.ent.size() * 4, sic.ent.data());
     add_seg(D.fac, S * std::max<std::size_t>(a8, 8), nullptr);

@@ -18,19 +18,20 @@
 // ----------------------------------------------------------
 // The reference sums each ring entry sequentially in ascending source order
 // (network.cpp:249-279).  Here every target owns one bit per incoming edge,
-// its in-edges sorted by (source, position in the source's row).  A spiking
-// source sets the bits of its out-edges in the arrival slot (integer
-// atomicOr, no return value needed) and bumps the target's pending count.
-// The target, when that slot arrives, walks its set bits in ascending order
-// and adds the contributions left to right: the same IEEE operations in the
-// same order as the reference, hence bitwise equal, for any number of
-// coincident spikes.
+// its in-edges sorted by (source, position in the source's row), in bitmap
+// words of its own.  A spiking source writes the value w*x*u of each out-edge
+// at that edge's bit position, sets the bit (integer atomicOr, no return
+// value), and sets the target's summary bit for the word group holding it
+// (64-bit summary per target and slot).  The target, when the slot arrives,
+// visits only the non-empty words its summary names, walks their set bits
+// in ascending order and adds the values left to right: the reference's IEEE
+// operations in the reference's order, hence bitwise equal, for any number
+// of coincident spikes.  Reading clears the summary and the words it used.
 //
 // STP: the reference keeps x, u, t_last per edge, but all edges of a source
 // start equal (network.cpp:43-52) and are updated together on each spike of
 // that source, so they stay equal: one state per source is exact.  The
-// spiking thread updates it and stores the post-spike (x, u) in a snapshot
-// row of its emission slot, from which the receivers form w*x*u.
+// spiking thread updates it and forms w*x*u once per set.
 //
 // SIC: the reference adds w_a2n*factor(a) once per astrocyte->neuron edge, in
 // ascending astrocyte order (network.cpp:281-299).  A target's edges from one
@@ -58,16 +59,14 @@ struct Work {
 
 // Incoming-edge structure of one arrival ring (transpose of a source CSR).
 struct InRing {
-    const std::uint32_t* row;     // [n_targets+1] start of each target's in-list
-    const std::uint32_t* src;     // [E] source of each in-edge (sorted per target)
     const std::uint32_t* wbase;   // [n_targets+1] first bitmap word of each target
     const std::uint32_t* bitpos;  // [E] bit index of each OUT-edge (source CSR order)
-    std::uint32_t* bits;          // [slots][total words] arrival bitmaps
-    std::uint32_t* cnt;           // [slots][n_targets] set bits pending per target
+    const std::uint8_t* sbit;     // [E] summary bit of that edge's word group
+    std::uint32_t* bits;          // [slots][words] arrival bitmaps
+    unsigned long long* sum;      // [slots][n_targets] non-empty word groups
+    double* vals;                 // [slots][words*32] value at each set bit
     std::uint32_t words;          // total bitmap words of one slot
     std::uint32_t n_targets;
-    std::uint32_t src_base;       // global neuron index of local source 0
-    std::uint32_t pad;
 };
 
 struct InstDev {
@@ -99,9 +98,8 @@ struct InstDev {
     // astrocyte state / params
     double *Ca, *IP3, *h;
     const double *Ca_tot, *IP3_0, *tau, *delta;
-    // STP per source + per-slot snapshots of (x, u) at emission
+    // STP per source
     double *stp_x, *stp_u, *stp_t;
-    double *snap_x, *snap_u;  // [slots][N]
     // out-edge CSR (source order) of the three spike-carrying sets
     const std::uint32_t *exc_rs, *exc_tg, *inh_rs, *inh_tg, *n2a_rs, *n2a_tg;
     InRing ring_ex, ring_in, ring_as;

@@ -27,34 +27,34 @@ __device__ __forceinline__ void add_syn(double v, double& exc_in, double& inh_in
 // Ordered sum of one target's arrivals in `slot` (see asg_engine.cuh).
 // kSubtract selects ring_inh's `-=` accumulation (network.cpp:271-275).
 template <bool kSubtract>
-__device__ __forceinline__ double ring_sum(const InstDev& I, const InRing& R, int slot,
-                                           std::uint32_t t, std::int64_t emit_step,
-                                           double weight) {
-    std::uint32_t* cnt = R.cnt + static_cast<std::size_t>(slot) * R.n_targets + t;
-    const std::uint32_t n = *cnt;
-    if (n == 0) return 0.0;
-    *cnt = 0;
-    const std::size_t snap = static_cast<std::size_t>(emit_step % I.slots) * I.N;
+__device__ __forceinline__ double ring_sum(const InRing& R, int slot, std::uint32_t t) {
+    unsigned long long* sp = R.sum + static_cast<std::size_t>(slot) * R.n_targets + t;
+    unsigned long long groups = *sp;
+    if (groups == 0) return 0.0;
+    *sp = 0;
     std::uint32_t* bits = R.bits + static_cast<std::size_t>(slot) * R.words;
-    const std::uint32_t w0 = R.wbase[t], w1 = R.wbase[t + 1];
-    const std::uint32_t* src = R.src + R.row[t];
+    const double* vals = R.vals + static_cast<std::size_t>(slot) * R.words * 32;
+    const std::uint32_t w0 = R.wbase[t], nw = R.wbase[t + 1] - w0;
+    const std::uint32_t G = (nw + 63) >> 6;  // words per summary bit
     double acc = 0.0;
-    std::uint32_t seen = 0;
-    for (std::uint32_t q = w0; q < w1 && seen < n; ++q) {
-        std::uint32_t word = bits[q];
-        if (word == 0) continue;
-        bits[q] = 0;
-        while (word != 0) {
-            const int b = __ffs(word) - 1;
-            word &= word - 1;
-            const std::uint32_t j = R.src_base + src[(q - w0) * 32 + b];
-            const double c = I.stp_on ? weight * I.snap_x[snap + j] * I.snap_u[snap + j] : weight;
-            if (kSubtract) {
-                acc -= c;
-            } else {
-                acc += c;
+    while (groups != 0) {
+        const std::uint32_t g = __ffsll(groups) - 1;
+        groups &= groups - 1;
+        const std::uint32_t q0 = w0 + g * G, q1 = min(q0 + G, w0 + nw);
+        for (std::uint32_t q = q0; q < q1; ++q) {
+            std::uint32_t word = bits[q];
+            if (word == 0) continue;
+            bits[q] = 0;
+            while (word != 0) {
+                const int b = __ffs(word) - 1;
+                word &= word - 1;
+                const double c = vals[static_cast<std::size_t>(q) * 32 + b];
+                if (kSubtract) {
+                    acc -= c;
+                } else {
+                    acc += c;
+                }
             }
-            ++seen;
         }
     }
     return acc;
@@ -82,22 +82,28 @@ __device__ __forceinline__ double sic_sum(const InstDev& I, std::uint32_t t, int
     return acc;
 }
 
+// Writes `value` at the bit of each out-edge of `row` in `slot`, sets the
+// bit and the target's summary bit.
 __device__ __forceinline__ void push_row(const std::uint32_t* rs, const std::uint32_t* tg,
-                                         const InRing& R, std::uint32_t row, int slot) {
+                                         const InRing& R, std::uint32_t row, int slot,
+                                         double value) {
     std::uint32_t* bits = R.bits + static_cast<std::size_t>(slot) * R.words;
-    std::uint32_t* cnt = R.cnt + static_cast<std::size_t>(slot) * R.n_targets;
+    unsigned long long* sum = R.sum + static_cast<std::size_t>(slot) * R.n_targets;
+    double* vals = R.vals + static_cast<std::size_t>(slot) * R.words * 32;
     const std::uint32_t e1 = rs[row + 1];
 #pragma unroll 4
     for (std::uint32_t e = rs[row] + threadIdx.x; e < e1; e += blockDim.x) {
         const std::uint32_t t = tg[e];
         const std::uint32_t b = R.bitpos[e];
+        vals[b] = value;
         atomicOr(bits + (b >> 5), 1u << (b & 31));
-        atomicAdd(cnt + t, 1u);
+        atomicOr(sum + t, 1ull << R.sbit[e]);
     }
 }
 
 __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step) {
     __shared__ std::uint32_t s_spk[kMaxBlock];
+    __shared__ double s_val[2 * kMaxBlock];
     __shared__ int s_nspk;
     if (threadIdx.x == 0) s_nspk = 0;
     __syncthreads();
@@ -111,9 +117,9 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
         // apply_arrivals (network.cpp:301-338)
         double exc_in = 0.0, inh_in = 0.0;
         {
-            const double ex = ring_sum<false>(I, I.ring_ex, slot, c, step - I.d_e, I.w_e);
+            const double ex = ring_sum<false>(I.ring_ex, slot, c);
             if (ex != 0.0) add_syn(ex, exc_in, inh_in);
-            const double in = ring_sum<true>(I, I.ring_in, slot, c, step - I.d_i, I.w_i);
+            const double in = ring_sum<true>(I.ring_in, slot, c);
             if (in != 0.0) add_syn(-in, exc_in, inh_in);
         }
         double Isic = I.Isic[c];
@@ -200,24 +206,27 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
         I.refr[c] = refr;
 
         if (spiked) {
-            // Tsodyks-Markram update of this source (network.cpp:230-247)
+            // Tsodyks-Markram update of this source (network.cpp:230-247); the
+            // value its edges deliver is w*x*u per set.
+            double x = 1.0, u = 1.0;
             if (I.stp_on) {
                 const double t_now = static_cast<double>(step) * I.dt;
                 const double d = t_now - I.stp_t[c];
                 const double xd = exp(-d / I.tau_rec);
                 const double ud = I.tau_fac < 1e-10 ? 0.0 : exp(-d / I.tau_fac);
-                double x = I.stp_x[c], u = I.stp_u[c];
+                x = I.stp_x[c];
+                u = I.stp_u[c];
                 x = 1.0 + (x - x * u - 1.0) * xd;
                 u = I.U + u * (1.0 - I.U) * ud;
                 I.stp_x[c] = x;
                 I.stp_u[c] = u;
                 I.stp_t[c] = t_now;
-                const std::size_t sn = static_cast<std::size_t>(slot) * I.N + c;
-                I.snap_x[sn] = x;
-                I.snap_u[sn] = u;
             }
+            s_val[threadIdx.x * 2 + 0] =
+                exc ? (I.stp_on ? I.w_e * x * u : I.w_e) : (I.stp_on ? I.w_i * x * u : I.w_i);
+            s_val[threadIdx.x * 2 + 1] = exc ? (I.stp_on ? I.w_n2a * x * u : I.w_n2a) : 0.0;
             const int pos = atomicAdd(&s_nspk, 1);
-            s_spk[pos] = c;
+            s_spk[pos] = threadIdx.x;
             if (I.rec_spikes && step >= I.rec_from) {
                 const unsigned long long li = atomicAdd(I.spike_log_n, 1ULL);
                 if (li < I.spike_log_cap) {
@@ -247,14 +256,15 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
     __syncthreads();
     const int nspk = s_nspk;
     for (int q = 0; q < nspk; ++q) {
-        const std::uint32_t j = s_spk[q];
+        const std::uint32_t lane = s_spk[q];
+        const std::uint32_t j = wk.first + lane;
         if (j < I.NE) {
             const int as = static_cast<int>((step + I.d_e) % I.slots);
-            push_row(I.exc_rs, I.exc_tg, I.ring_ex, j, as);
-            push_row(I.n2a_rs, I.n2a_tg, I.ring_as, j, as);
+            push_row(I.exc_rs, I.exc_tg, I.ring_ex, j, as, s_val[2 * lane]);
+            push_row(I.n2a_rs, I.n2a_tg, I.ring_as, j, as, s_val[2 * lane + 1]);
         } else {
             const int as = static_cast<int>((step + I.d_i) % I.slots);
-            push_row(I.inh_rs, I.inh_tg, I.ring_in, j - I.NE, as);
+            push_row(I.inh_rs, I.inh_tg, I.ring_in, j - I.NE, as, s_val[2 * lane]);
         }
     }
 }
@@ -265,7 +275,7 @@ __device__ void astro_role(const InstDev& I, const Work& wk, std::int64_t step) 
     const int slot = static_cast<int>(step % I.slots);
     double ip3_in = 0.0;
     {
-        const double v = ring_sum<false>(I, I.ring_as, slot, a, step - I.d_e, I.w_n2a);
+        const double v = ring_sum<false>(I.ring_as, slot, a);
         if (v != 0.0) ip3_in += v;
     }
     // drive_astrocytes (network.cpp:340-355)
