@@ -105,10 +105,8 @@ class State(C.Structure):
 
 
 class EngineOpts(C.Structure):
-    _fields_ = [("device", C.c_int32), ("chunk_steps", C.c_int32),
-                ("block_neuron", C.c_int32), ("block_astro", C.c_int32),
-                ("block_sic", C.c_int32), ("claim_slots", C.c_int32),
-                ("use_graphs", C.c_int32), ("sic_mode", C.c_int32),
+    _fields_ = [("device", C.c_int32), ("chunk_steps", C.c_int32), ("block", C.c_int32),
+                ("use_graphs", C.c_int32), ("sic_mode", C.c_int32), ("pdl", C.c_int32),
                 ("mem_budget", C.c_uint64)]
 
 
@@ -185,6 +183,8 @@ SIGNATURES = {
                                           C.c_double]),
     "asg_astro_pull_state": (C.c_int, [vp, c_double_p, c_double_p, c_double_p]),
     "asg_astro_last_timing": (C.c_int, [vp, c_double_p, c_int64_p]),
+    "asg_astro_autotune": (C.c_int, [vp, c_double_p, C.c_double, C.c_int32, C.c_int32,
+                                     c_int32_p, c_double_p]),
     # host config + builder
     "asg_model_from_json": (C.c_int, [C.c_char_p, C.c_int64, C.c_double, C.c_double, C.c_int64,
                                       vpp]),

@@ -118,6 +118,14 @@ class AstroBackend:
         _lib.call("asg_astro_last_timing", self._h, C.byref(ms), C.byref(k))
         return ms.value, k.value
 
+    def autotune(self, w: ScalingWorkload, steps=20):
+        """Pick the fastest launch shape on a scratch copy (state unchanged)."""
+        chosen = C.c_int32()
+        us = C.c_double()
+        _lib.call("asg_astro_autotune", self._h, _lib.dptr(w.consts), w.h_step, w.substeps,
+                  int(steps), C.byref(chosen), C.byref(us))
+        return chosen.value, us.value
+
     def destroy(self):
         if self._h:
             out = [np.empty(self.n, dtype=np.float64) for _ in range(3)]

@@ -16,10 +16,10 @@ EngineConfig config_from(const asg_engine_opts* o) {
     if (o != nullptr) {
         c.device = o->device;
         if (o->chunk_steps > 0) c.chunk_steps = o->chunk_steps;
-        const int b = o->block_neuron > 0 ? o->block_neuron : 0;
-        if (b > 0) c.block = b;
+        if (o->block > 0) c.block = o->block;
         if (o->use_graphs != 0) c.use_graphs = o->use_graphs;
         c.sic_mode = o->sic_mode;
+        c.pdl = o->pdl >= 0;
         c.mem_budget = o->mem_budget;
     }
     return c;
@@ -385,7 +385,7 @@ int asg_batch_autotune(asg_batch* b, int32_t steps, asg_engine_opts* chosen) {
         std::memset(chosen, 0, sizeof *chosen);
         chosen->device = e.cfg.device;
         chosen->chunk_steps = best_chunk;
-        chosen->block_neuron = chosen->block_astro = chosen->block_sic = best_block;
+        chosen->block = best_block;
         chosen->use_graphs = e.cfg.use_graphs;
         chosen->sic_mode = e.cfg.sic_mode;
         chosen->mem_budget = e.cfg.mem_budget;

@@ -86,36 +86,79 @@ __device__ __forceinline__ void advance_cell(const StepArgs& a, const AstroArray
     }
 }
 
-template <bool kUniform, int kInput, bool kNoise>
-__global__ void __launch_bounds__(128, 4) astro_step_kernel(StepArgs a, AstroArrays s) {
+// kCells adjacent cells per thread (1: 64-bit accesses, 2: 128-bit accesses
+// and two interleaved RK4 chains); kMinBlocks sets the register budget
+// through __launch_bounds__ (65536 / (kBlock * kMinBlocks) per thread).
+template <bool kUniform, int kInput, bool kNoise, int kCells, int kBlock, int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) astro_step_kernel(StepArgs a, AstroArrays s) {
     const std::int64_t step =
         (kInput == kInputBernoulli) ? (*a.step_base + a.step_offset) : 0;
-    const std::int64_t pairs = a.n / 2;
     const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
-    double2* Ca2 = reinterpret_cast<double2*>(s.Ca);
-    double2* IP32 = reinterpret_cast<double2*>(s.IP3);
-    double2* h2 = reinterpret_cast<double2*>(s.h);
-    for (std::int64_t p = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-         p < pairs; p += stride) {
-        double2 ca = Ca2[p], ip3 = IP32[p], hh = h2[p];
-        const std::int64_t i = 2 * p;
-        advance_cell<kUniform, kInput, kNoise>(a, s, i, step, ca.x, ip3.x, hh.x);
-        advance_cell<kUniform, kInput, kNoise>(a, s, i + 1, step, ca.y, ip3.y, hh.y);
-        Ca2[p] = ca;
-        IP32[p] = ip3;
-        h2[p] = hh;
-        if (kInput == kInputArray) reinterpret_cast<double2*>(s.input)[p] = make_double2(0.0, 0.0);
+    if (kCells == 2) {
+        const std::int64_t pairs = a.n / 2;
+        double2* Ca2 = reinterpret_cast<double2*>(s.Ca);
+        double2* IP32 = reinterpret_cast<double2*>(s.IP3);
+        double2* h2 = reinterpret_cast<double2*>(s.h);
+        for (std::int64_t p = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+             p < pairs; p += stride) {
+            double2 ca = Ca2[p], ip3 = IP32[p], hh = h2[p];
+            const std::int64_t i = 2 * p;
+            advance_cell<kUniform, kInput, kNoise>(a, s, i, step, ca.x, ip3.x, hh.x);
+            advance_cell<kUniform, kInput, kNoise>(a, s, i + 1, step, ca.y, ip3.y, hh.y);
+            Ca2[p] = ca;
+            IP32[p] = ip3;
+            h2[p] = hh;
+            if (kInput == kInputArray)
+                reinterpret_cast<double2*>(s.input)[p] = make_double2(0.0, 0.0);
+        }
+        // Odd tail cell.
+        if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+            const std::int64_t i = a.n - 1;
+            double ca = s.Ca[i], ip3 = s.IP3[i], hh = s.h[i];
+            advance_cell<kUniform, kInput, kNoise>(a, s, i, step, ca, ip3, hh);
+            s.Ca[i] = ca;
+            s.IP3[i] = ip3;
+            s.h[i] = hh;
+            if (kInput == kInputArray) s.input[i] = 0.0;
+        }
+    } else {
+        for (std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+             i < a.n; i += stride) {
+            double ca = s.Ca[i], ip3 = s.IP3[i], hh = s.h[i];
+            advance_cell<kUniform, kInput, kNoise>(a, s, i, step, ca, ip3, hh);
+            s.Ca[i] = ca;
+            s.IP3[i] = ip3;
+            s.h[i] = hh;
+            if (kInput == kInputArray) s.input[i] = 0.0;
+        }
     }
-    // Odd tail cell.
-    if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
-        const std::int64_t i = a.n - 1;
-        double ca = s.Ca[i], ip3 = s.IP3[i], hh = s.h[i];
-        advance_cell<kUniform, kInput, kNoise>(a, s, i, step, ca, ip3, hh);
-        s.Ca[i] = ca;
-        s.IP3[i] = ip3;
-        s.h[i] = hh;
-        if (kInput == kInputArray) s.input[i] = 0.0;
+}
+
+// Launch shapes the autotuner chooses between (cells/thread, block, blocks/SM
+// the register budget allows).
+struct Shape {
+    int cells, block, min_blocks;
+};
+constexpr Shape kShapes[] = {{2, 128, 4}, {1, 128, 8}, {1, 256, 4}, {2, 128, 6},
+                             {1, 128, 6}, {1, 64, 12}};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+template <bool kUniform, int kInput, bool kNoise>
+cudaError_t launch_astro(int shape, int sms, StepArgs a, AstroArrays s, cudaStream_t st) {
+    const Shape sh = kShapes[shape];
+    const std::int64_t units = sh.cells == 2 ? std::max<std::int64_t>(1, a.n / 2) : a.n;
+    const std::int64_t want = (units + sh.block - 1) / sh.block;
+    const std::int64_t cap = static_cast<std::int64_t>(sms) * sh.min_blocks * 4;
+    const int grid = static_cast<int>(std::max<std::int64_t>(1, std::min(want, cap)));
+    switch (shape) {
+        case 0: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 4><<<grid, 128, 0, st>>>(a, s); break;
+        case 1: astro_step_kernel<kUniform, kInput, kNoise, 1, 128, 8><<<grid, 128, 0, st>>>(a, s); break;
+        case 2: astro_step_kernel<kUniform, kInput, kNoise, 1, 256, 4><<<grid, 256, 0, st>>>(a, s); break;
+        case 3: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 6><<<grid, 128, 0, st>>>(a, s); break;
+        case 4: astro_step_kernel<kUniform, kInput, kNoise, 1, 128, 6><<<grid, 128, 0, st>>>(a, s); break;
+        default: astro_step_kernel<kUniform, kInput, kNoise, 1, 64, 12><<<grid, 64, 0, st>>>(a, s); break;
     }
+    return cudaGetLastError();
 }
 
 __global__ void advance_counter_kernel(std::int64_t* base, std::int64_t by) { *base += by; }
@@ -152,9 +195,11 @@ struct AstroEngine {
     DevBuf Ca, IP3, h, input, Ca_tot, IP3_0, tau, delta, step_base;
     double last_ms = 0.0;
     std::int64_t last_kernels = 0;
+    int shape = 0;  // launch shape (see kShapes), set by asg_astro_autotune
     // Captured chunk of Bernoulli steps, rebuilt when its arguments change.
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
+    int graph_shape = -1;
     StepArgs graph_args{};
     bool graph_uniform = true;
 
@@ -305,20 +350,12 @@ int asg_astro_update(asg_astro* s, const double* consts, double h_step, int32_t 
     a.noise_seed = noise_seed;
     a.noise_index = noise_index;
     a.step_base = e->step_base.as<std::int64_t>();
-    const int block = 128;
-    const int grid = e->grid_for(std::max<std::int64_t>(1, e->n / 2), block);
     ASG_CUDA(cudaEventRecord(e->ev0, e->stream));
     // The reference applies noise only when noise_std > 0 (astrocyte.cpp:
-    // 313-322): otherwise the shared value (0) enters the RHS.
-    if (noise_std > 0.0) {
-        asg::astro_step_kernel<false, asg::kInputArray, true>
-            <<<grid, block, 0, e->stream>>>(a, e->arrays());
-    } else {
-        a.independent = 0;
-        asg::astro_step_kernel<false, asg::kInputArray, true>
-            <<<grid, block, 0, e->stream>>>(a, e->arrays());
-    }
-    ASG_CUDA(cudaGetLastError());
+    // 313-322); otherwise the caller's shared value (0) enters the RHS.
+    if (!(noise_std > 0.0)) a.independent = 0;
+    ASG_CUDA((asg::launch_astro<false, asg::kInputArray, true>(e->shape, e->sms, a,
+                                                                e->arrays(), e->stream)));
     ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
     e->last_kernels = 1;
     return ASG_OK;
@@ -350,25 +387,23 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
     a.p = p;
     a.weight = weight;
     a.step_base = e->step_base.as<std::int64_t>();
-    const int block = 128;
-    const int grid = e->grid_for(std::max<std::int64_t>(1, e->n / 2), block);
 
     // Steps run as captured chunks of up to 64 launches: kernel j of a chunk
     // reads step = *step_base + j, and a one-thread node advances the base.
     const int chunk = static_cast<int>(std::min<std::int64_t>(64, count));
+    cudaError_t launch_err = cudaSuccess;
     auto launch_step = [&](int j) {
         asg::StepArgs aj = a;
         aj.step_offset = j;
-        if (uniform) {
-            asg::astro_step_kernel<true, asg::kInputBernoulli, false>
-                <<<grid, block, 0, e->stream>>>(aj, e->arrays());
-        } else {
-            asg::astro_step_kernel<false, asg::kInputBernoulli, false>
-                <<<grid, block, 0, e->stream>>>(aj, e->arrays());
-        }
+        const cudaError_t le =
+            uniform ? asg::launch_astro<true, asg::kInputBernoulli, false>(e->shape, e->sms, aj,
+                                                                            e->arrays(), e->stream)
+                    : asg::launch_astro<false, asg::kInputBernoulli, false>(e->shape, e->sms, aj,
+                                                                             e->arrays(), e->stream);
+        if (le != cudaSuccess) launch_err = le;
     };
     const bool same = e->graph != nullptr && e->graph_steps == chunk &&
-                      e->graph_uniform == (uniform != 0) &&
+                      e->graph_uniform == (uniform != 0) && e->graph_shape == e->shape &&
                       std::memcmp(&e->graph_args, &a, sizeof a) == 0;
     if (!same) {
         if (e->graph) cudaGraphExecDestroy(e->graph);
@@ -376,6 +411,7 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
         cudaGraph_t g = nullptr;
         ASG_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
         for (int j = 0; j < chunk; ++j) launch_step(j);
+        ASG_CUDA(launch_err);
         asg::advance_counter_kernel<<<1, 1, 0, e->stream>>>(e->step_base.as<std::int64_t>(), chunk);
         ASG_CUDA(cudaStreamEndCapture(e->stream, &g));
         const cudaError_t ce = cudaGraphInstantiate(&e->graph, g, 0);
@@ -384,6 +420,7 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
         e->graph_steps = chunk;
         e->graph_args = a;
         e->graph_uniform = uniform != 0;
+        e->graph_shape = e->shape;
     }
     std::int64_t base = first;
     ASG_CUDA(cudaMemcpyAsync(e->step_base.get(), &base, sizeof base, cudaMemcpyHostToDevice, e->stream));
@@ -399,7 +436,7 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
     if (done < count) {
         // Remainder: plain launches with the base already advanced.
         for (int j = 0; done + j < count; ++j) launch_step(j);
-        ASG_CUDA(cudaGetLastError());
+        ASG_CUDA(launch_err);
         kernels += count - done;
     }
     ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
@@ -421,3 +458,60 @@ int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels) {
 }
 
 }  // extern "C"
+
+extern "C" int asg_astro_autotune(asg_astro* s, const double* consts, double h_step,
+                                  int32_t substeps, int32_t steps, int32_t* chosen,
+                                  double* us_per_step) {
+    asg::clear_error();
+    if (s == nullptr || consts == nullptr || steps <= 0)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_autotune: bad arguments");
+    auto* e = reinterpret_cast<AstroEngine*>(s);
+    if (e->n == 0) return ASG_OK;
+    const std::size_t bytes = static_cast<std::size_t>(e->n) * sizeof(double);
+    // Scratch copies of the state: the trials advance these, not the handle's.
+    asg::DevBuf ca, ip3, h;
+    ASG_TRY(ca.alloc(bytes, false));
+    ASG_TRY(ip3.alloc(bytes, false));
+    ASG_TRY(h.alloc(bytes, false));
+    ASG_CUDA(cudaMemcpyAsync(ca.get(), e->Ca.get(), bytes, cudaMemcpyDeviceToDevice, e->stream));
+    ASG_CUDA(cudaMemcpyAsync(ip3.get(), e->IP3.get(), bytes, cudaMemcpyDeviceToDevice, e->stream));
+    ASG_CUDA(cudaMemcpyAsync(h.get(), e->h.get(), bytes, cudaMemcpyDeviceToDevice, e->stream));
+    asg::AstroArrays arr = e->arrays();
+    arr.Ca = ca.as<double>();
+    arr.IP3 = ip3.as<double>();
+    arr.h = h.as<double>();
+    asg::StepArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n = e->n;
+    a.k = asg::make_astro_k(consts, h_step, substeps);
+    a.u = asg::UniformParams{1.8958264782990153, 0.010925583871830699, 1058.7589568400845,
+                             0.04911592657233997};
+    a.seed = 1;
+    a.p = 0.01;
+    a.weight = 0.2;
+    a.step_base = e->step_base.as<std::int64_t>();
+    int best = e->shape;
+    float best_ms = 1e30f;
+    for (int shape = 0; shape < asg::kNumShapes; ++shape) {
+        for (int rep = 0; rep < 2; ++rep) {  // first pass warms up
+            ASG_CUDA(cudaEventRecord(e->ev0, e->stream));
+            for (int j = 0; j < steps; ++j) {
+                a.step_offset = j;
+                ASG_CUDA((asg::launch_astro<true, asg::kInputBernoulli, false>(shape, e->sms, a,
+                                                                                arr, e->stream)));
+            }
+            ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
+            ASG_CUDA(cudaEventSynchronize(e->ev1));
+        }
+        float ms = 0.0f;
+        ASG_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = shape;
+        }
+    }
+    e->shape = best;
+    if (chosen) *chosen = best;
+    if (us_per_step) *us_per_step = 1e3 * best_ms / steps;
+    return ASG_OK;
+}

@@ -616,10 +616,15 @@ int Engine::rebuild() {
     if (cfg.use_graphs >= 0 && !work.empty()) {
         cudaGraph_t g = nullptr;
         ASG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < cfg.chunk_steps; ++k)
-            launch_step(d_insts.as<InstDev>(), d_work.as<Work>(), static_cast<int>(work.size()),
-                        B, k, stream);
+        cudaError_t le = cudaSuccess;
+        for (int k = 0; k < cfg.chunk_steps && le == cudaSuccess; ++k)
+            le = launch_step(d_insts.as<InstDev>(), d_work.as<Work>(),
+                             static_cast<int>(work.size()), B, k, cfg.pdl, stream);
         const cudaError_t ce = cudaStreamEndCapture(stream, &g);
+        if (le != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(le, "step launch (capture)", __FILE__, __LINE__);
+        }
         if (ce != cudaSuccess) return cuda_fail(ce, "graph capture", __FILE__, __LINE__);
         const cudaError_t ci = cudaGraphInstantiate(&graph, g, 0);
         cudaGraphDestroy(g);
@@ -659,9 +664,8 @@ int Engine::launch_chunk(int parity, int steps) {
         ASG_CUDA(cudaGraphLaunch(graph, stream));
     } else {
         for (int k = 0; k < steps; ++k)
-            launch_step(d_insts.as<InstDev>(), d_work.as<Work>(), static_cast<int>(work.size()),
-                        cfg.block, k, stream);
-        ASG_CUDA(cudaGetLastError());
+            ASG_CUDA(launch_step(d_insts.as<InstDev>(), d_work.as<Work>(),
+                                 static_cast<int>(work.size()), cfg.block, k, cfg.pdl, stream));
     }
     last_kernels += steps;
     launched_kernels += steps;

@@ -120,7 +120,10 @@ struct InstDev {
     unsigned long long* counters;  // spike_edges, sic_edges, spikes, overflow
 };
 
-void launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
-                 cudaStream_t stream);
+// One step launch; with `pdl` the launch may start while the previous kernel
+// of the stream is still running (the kernel waits for it before any access
+// to instance state).
+cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
+                        bool pdl, cudaStream_t stream);
 
 }  // namespace asg

@@ -57,6 +57,7 @@ struct EngineConfig {
     int block = 128;
     int use_graphs = 1;
     int sic_mode = 0;  // 0 auto, 1 fused, 2 split
+    bool pdl = true;   // programmatic dependent launch between steps
     std::uint64_t mem_budget = 0;
 };
 

@@ -24,44 +24,83 @@ __device__ __forceinline__ void add_syn(double v, double& exc_in, double& inh_in
     }
 }
 
-// Ordered sum of one target's arrivals in `slot` (see asg_engine.cuh).
+// Ordered sum of one target's arrivals in `slot` (see asg_engine.cuh), given
+// the summary word already read (and cleared) by the caller.  Loads are
+// issued in batches of independent requests -- up to 8 bitmap words, then up
+// to 8 values -- so a target with several arrivals pays a few memory round
+// trips, not one per arrival; the additions stay in ascending bit order.
 // kSubtract selects ring_inh's `-=` accumulation (network.cpp:271-275).
 template <bool kSubtract>
-__device__ __forceinline__ double ring_sum(const InRing& R, int slot, std::uint32_t t) {
-    unsigned long long* sp = R.sum + static_cast<std::size_t>(slot) * R.n_targets + t;
-    unsigned long long groups = *sp;
-    if (groups == 0) return 0.0;
-    *sp = 0;
+__device__ __forceinline__ double ring_gather(const InRing& R, int slot, std::uint32_t t,
+                                              unsigned long long groups) {
     std::uint32_t* bits = R.bits + static_cast<std::size_t>(slot) * R.words;
     const double* vals = R.vals + static_cast<std::size_t>(slot) * R.words * 32;
     const std::uint32_t w0 = R.wbase[t], nw = R.wbase[t + 1] - w0;
     const std::uint32_t G = (nw + 63) >> 6;  // words per summary bit
     double acc = 0.0;
-    while (groups != 0) {
-        const std::uint32_t g = __ffsll(groups) - 1;
-        groups &= groups - 1;
-        const std::uint32_t q0 = w0 + g * G, q1 = min(q0 + G, w0 + nw);
-        for (std::uint32_t q = q0; q < q1; ++q) {
-            std::uint32_t word = bits[q];
-            if (word == 0) continue;
-            bits[q] = 0;
-            while (word != 0) {
-                const int b = __ffs(word) - 1;
-                word &= word - 1;
-                const double c = vals[static_cast<std::size_t>(q) * 32 + b];
+    std::uint32_t idx[8];
+    int n = 0;
+    auto flush = [&]() {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = k < n ? vals[idx[k]] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k < n) {
                 if (kSubtract) {
-                    acc -= c;
+                    acc -= v[k];
                 } else {
-                    acc += c;
+                    acc += v[k];
                 }
             }
         }
+        n = 0;
+    };
+    auto take_word = [&](std::uint32_t q, std::uint32_t word) {
+        while (word != 0) {
+            const int b = __ffs(word) - 1;
+            word &= word - 1;
+            idx[n++] = q * 32 + b;
+            if (n == 8) flush();
+        }
+    };
+    // Word groups in ascending order, up to 8 words loaded at once.
+    std::uint32_t q[8], wv[8];
+    std::uint32_t cur = 0, cur_end = 0;  // words [cur, cur_end) of the open group
+    bool open = false;
+    for (;;) {
+        int nq = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (!open && groups != 0) {
+                const std::uint32_t g = __ffsll(groups) - 1;
+                groups &= groups - 1;
+                cur = w0 + g * G;
+                cur_end = min(cur + G, w0 + nw);
+                open = cur < cur_end;
+            }
+            q[k] = cur;
+            if (open) {
+                nq = k + 1;
+                if (++cur >= cur_end) open = false;
+            }
+        }
+        if (nq == 0) break;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) wv[k] = k < nq ? bits[q[k]] : 0u;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (k < nq && wv[k] != 0) bits[q[k]] = 0;
+        for (int k = 0; k < nq; ++k) take_word(q[k], wv[k]);
     }
+    flush();
     return acc;
 }
 
 // Sequential SIC sum of target t from the factors of emission slot fslot
-// (network.cpp:281-299 order: ascending astrocyte, one add per edge).
+// (network.cpp:281-299 order: ascending astrocyte, one add per edge).  The
+// list entries and their factors are fetched 8 at a time with independent
+// loads before the dependent additions.
 __device__ __forceinline__ double sic_sum(const InstDev& I, std::uint32_t t, int fslot,
                                           unsigned long long& edges) {
     const std::uint32_t slice = t >> 5, lane = t & 31;
@@ -69,15 +108,22 @@ __device__ __forceinline__ double sic_sum(const InstDev& I, std::uint32_t t, int
     const std::uint32_t len = (o1 - o0) >> 5;
     const double* fac = I.fac + static_cast<std::size_t>(fslot) * I.NA;
     double acc = 0.0;
-    for (std::uint32_t q = 0; q < len; ++q) {
-        const std::uint32_t e = I.sic_ent[o0 + q * 32 + lane];
-        const std::uint32_t m = e & 0xFFu;
-        if (m == 0) break;  // padding ends the list
-        const double f = fac[e >> 8];
-        if (f == 0.0) continue;
-        const double c = I.w_a2n * f;
-        for (std::uint32_t r = 0; r < m; ++r) acc += c;
-        edges += m;
+    for (std::uint32_t b0 = 0; b0 < len; b0 += 8) {
+        std::uint32_t e[8];
+        double f[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) e[k] = b0 + k < len ? __ldg(I.sic_ent + o0 + (b0 + k) * 32 + lane) : 0u;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) f[k] = (e[k] & 0xFFu) ? fac[e[k] >> 8] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const std::uint32_t m = e[k] & 0xFFu;
+            if (m == 0) return acc;  // padding ends the list
+            if (f[k] == 0.0) continue;
+            const double c = I.w_a2n * f[k];
+            for (std::uint32_t r = 0; r < m; ++r) acc += c;
+            edges += m;
+        }
     }
     return acc;
 }
@@ -114,23 +160,38 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
         const NeuronK& P = exc ? I.pe : I.pi;
         const int slot = static_cast<int>(step % I.slots);
 
+        // Issue every independent load of this cell before any store.
+        const std::size_t so = static_cast<std::size_t>(slot);
+        unsigned long long* sp_ex = I.ring_ex.sum + so * I.ring_ex.n_targets + c;
+        unsigned long long* sp_in = I.ring_in.sum + so * I.ring_in.n_targets + c;
+        const unsigned long long g_ex = *sp_ex, g_in = *sp_in;
+        const std::int64_t se = step - I.d_a2n;
+        const bool sic_due = se >= 0 && se % I.sic_interval == 0;
+        double Isic = (sic_due && !I.fused_sic)
+                          ? I.sic_val[static_cast<std::size_t>(step & 1) * I.N + c]
+                          : I.Isic[c];
+        double V = I.V[c], w = I.w[c], gex = I.gex[c], gin = I.gin[c];
+        double dgex = I.dgex[c], dgin = I.dgin[c];
+        int refr = I.refr[c];
+        const double Vr = I.V_reset[c], bc = I.b[c];
+
         // apply_arrivals (network.cpp:301-338)
         double exc_in = 0.0, inh_in = 0.0;
-        {
-            const double ex = ring_sum<false>(I.ring_ex, slot, c);
+        if (g_ex != 0) {
+            *sp_ex = 0;
+            const double ex = ring_gather<false>(I.ring_ex, slot, c, g_ex);
             if (ex != 0.0) add_syn(ex, exc_in, inh_in);
-            const double in = ring_sum<true>(I.ring_in, slot, c);
+        }
+        if (g_in != 0) {
+            *sp_in = 0;
+            const double in = ring_gather<true>(I.ring_in, slot, c, g_in);
             if (in != 0.0) add_syn(-in, exc_in, inh_in);
         }
-        double Isic = I.Isic[c];
-        const std::int64_t se = step - I.d_a2n;
-        if (se >= 0 && se % I.sic_interval == 0) {
+        if (sic_due) {
             if (I.fused_sic) {
                 unsigned long long edges = 0;
                 Isic = sic_sum(I, c, static_cast<int>(se % I.slots), edges);
                 if (edges) atomicAdd(I.counters + 1, edges);
-            } else {
-                Isic = I.sic_val[static_cast<std::size_t>(step & 1) * I.N + c];
             }
             I.Isic[c] = Isic;
         }
@@ -154,13 +215,9 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
             }
         }
 
-        double dgex = I.dgex[c], dgin = I.dgin[c];
         if (exc_in != 0.0) dgex += exc_in * P.psc_ex;
         if (inh_in != 0.0) dgin += inh_in * P.psc_in;
 
-        double V = I.V[c], w = I.w[c], gex = I.gex[c], gin = I.gin[c];
-        int refr = I.refr[c];
-        const double Vr = I.V_reset[c];
         const double h = I.ak.h;  // h_step is shared by both models
         const double half_h = I.ak.half_h, h6 = I.ak.h6;
         bool spiked = false;
@@ -192,7 +249,7 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
                 --refr;
             } else if (V >= P.V_peak) {
                 V = Vr;
-                w += I.b[c];
+                w += bc;
                 refr = P.ref_steps;
                 spiked = true;
             }
@@ -273,9 +330,13 @@ __device__ void astro_role(const InstDev& I, const Work& wk, std::int64_t step) 
     if (threadIdx.x >= wk.count) return;
     const std::uint32_t a = wk.first + threadIdx.x;
     const int slot = static_cast<int>(step % I.slots);
+    unsigned long long* sp = I.ring_as.sum + static_cast<std::size_t>(slot) * I.ring_as.n_targets + a;
+    const unsigned long long g = *sp;
+    double ca = I.Ca[a], ip3 = I.IP3[a], hh = I.h[a];
     double ip3_in = 0.0;
-    {
-        const double v = ring_sum<false>(I.ring_as, slot, a);
+    if (g != 0) {
+        *sp = 0;
+        const double v = ring_gather<false>(I.ring_as, slot, a, g);
         if (v != 0.0) ip3_in += v;
     }
     // drive_astrocytes (network.cpp:340-355)
@@ -292,7 +353,6 @@ __device__ void astro_role(const InstDev& I, const Work& wk, std::int64_t step) 
         noise = I.a_indep ? I.a_std * normal_clamped(nseed, idx * kStreamStride + a)
                           : I.a_std * normal_clamped(nseed, idx);
     }
-    double ca = I.Ca[a], ip3 = I.IP3[a], hh = I.h[a];
     if (I.astro_uniform) {
         astro_rk4(I.ak, I.Ca_tot_u, I.IP3_0_u, I.tau_u, I.delta_u, ip3_in, noise, ca, ip3, hh);
     } else {
@@ -346,6 +406,12 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restri
     }
     __syncthreads();
     const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
+    // Programmatic dependent launch: let the next step's grid be scheduled
+    // now, and wait here until the previous step's grid has completed and
+    // its memory is visible.  The descriptor and work table read above were
+    // written before the chunk started.
+    asm volatile("griddepcontrol.launch_dependents;");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const std::int64_t step = I.step0 + k;
     if (step >= I.end_step) return;
     if (wk.role == kRoleNeuron) {
@@ -359,9 +425,19 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restri
 
 }  // namespace
 
-void launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
-                 cudaStream_t stream) {
-    step_kernel<<<n_work, block, 0, stream>>>(insts, work, k);
+cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
+                        bool pdl, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(n_work));
+    cfg.blockDim = dim3(static_cast<unsigned>(block));
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = pdl ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, step_kernel, insts, work, k);
 }
 
 }  // namespace asg

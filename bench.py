@@ -159,6 +159,7 @@ def bench_astro_scaling(args, rank, world, pg):
     w = ScalingWorkload(n, seed=1 + rank)
     Ca, IP3, h = w.initial_state()
     eng = AstroBackend(Ca, IP3, h)
+    shape, tuned_us = eng.autotune(w, steps=10)
     # warm-up (untimed)
     step = 0
     for _ in range(args.warmup):
@@ -232,6 +233,7 @@ def bench_astro_scaling(args, rank, world, pg):
                      "bytes_per_launch": BYTES_PER_CELL_STEP * n,
                      "kernel": "astro_step_kernel<uniform,bernoulli>"},
         "clocks": clk.summary(),
+        "launch_shape": shape,
     }
     return out, (w, Ca, IP3, h)
 
@@ -484,6 +486,7 @@ def main():
                        "l2": "working set 24 B/cell = 240 MB > 126 MB L2 (no flush needed)"},
             "e2e": res["e2e"], "gpu_launches": res["kernels"], "roofline": res["roofline"],
             "clocks": res["clocks"], "per_launch_us": res["per_launch_us"],
+            "launch_shape": res["launch_shape"],
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu

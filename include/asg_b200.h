@@ -147,15 +147,13 @@ typedef struct asg_state {
 
 /* Engine options.  Zero-initialised fields take the defaults. */
 typedef struct asg_engine_opts {
-    int32_t device;         /* CUDA device ordinal (default 0)                 */
-    int32_t chunk_steps;    /* steps per captured CUDA graph (default 32)       */
-    int32_t block_neuron;   /* threads per block, neuron role (default 128)     */
-    int32_t block_astro;    /* threads per block, astrocyte role (default 128)  */
-    int32_t block_sic;      /* threads per block, SIC role (default 128)        */
-    int32_t claim_slots;    /* arrival entries kept per cell per ring slot (8)  */
-    int32_t use_graphs;     /* 1 = CUDA graphs (default), -1 = plain launches   */
-    int32_t sic_mode;       /* 0 auto, 1 fused into neuron, 2 separate role     */
-    uint64_t mem_budget;    /* device bytes the engine may hold (0 = 90% free)  */
+    int32_t device;         /* CUDA device ordinal (default 0)                    */
+    int32_t chunk_steps;    /* steps per captured CUDA graph (default 32)          */
+    int32_t block;          /* threads per block of the step kernel (default 128)  */
+    int32_t use_graphs;     /* 0/1 = CUDA graphs (default), -1 = plain launches    */
+    int32_t sic_mode;       /* 0 auto, 1 fused into the neuron role, 2 own role    */
+    int32_t pdl;            /* 0 = programmatic dependent launch (default), -1 off */
+    uint64_t mem_budget;    /* device bytes the engine may hold (0 = 90% free)     */
 } asg_engine_opts;
 
 /* ------------------------------------------------------ single network
@@ -282,6 +280,12 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
                             double delta_IP3);
 /* Read the state without destroying the handle. */
 int asg_astro_pull_state(asg_astro* s, double* Ca, double* IP3, double* h);
+/* Time the kernel's launch shapes (cells per thread, block size, register
+ * budget) for `steps` steps of the Bernoulli workload on a scratch copy of
+ * the state, keep the fastest for this handle (state unchanged) and return
+ * its index and per-step microseconds (may be NULL). */
+int asg_astro_autotune(asg_astro* s, const double* consts, double h_step, int32_t substeps,
+                       int32_t steps, int32_t* chosen, double* us_per_step);
 /* Device ms of the last run call and kernels launched. */
 int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels);
 

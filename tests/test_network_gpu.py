@@ -138,8 +138,8 @@ def test_sic_modes_and_block_sizes_bitwise():
     path = config_path("use_case")
     m = Model(path, pre_time=0.0)
     outs = []
-    for opts in (dict(sic_mode=1, block_neuron=64), dict(sic_mode=2, block_neuron=256),
-                 dict(sic_mode=0, block_neuron=128, chunk_steps=7, use_graphs=-1)):
+    for opts in (dict(sic_mode=1, block=64), dict(sic_mode=2, block=256),
+                 dict(sic_mode=0, block=128, chunk_steps=7, use_graphs=-1)):
         n = Network(m, record=rec_all(), **opts)
         n.step(1200)
         outs.append((n.fetch_spikes(), n.state()))
