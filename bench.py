@@ -55,7 +55,11 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled around the timed region.
+
+    The sampler is started and its first sample awaited before the timed
+    region begins; samples taken from that point until it stops are kept
+    (line-buffered output, 20 ms period)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -65,16 +69,24 @@ class ClockSampler:
         self.dev = device_index
         self.proc = None
         self.lines = []
+        self.error = None
 
     def __enter__(self):
+        import shutil
+        cmd = ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+               "--format=csv,noheader,nounits", "-lms", "20"]
+        if shutil.which("stdbuf"):
+            cmd = ["stdbuf", "-oL"] + cmd
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                         text=True, bufsize=1)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
-        except Exception:
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+        except Exception as e:  # noqa: BLE001
+            self.error = str(e)
             self.proc = None
         return self
 
@@ -84,11 +96,17 @@ class ClockSampler:
 
     def __exit__(self, *exc):
         if self.proc is not None:
+            time.sleep(0.05)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+            if not self.lines:
+                try:
+                    self.error = self.proc.stderr.read()[:200]
+                except Exception:
+                    pass
 
     def summary(self):
         sm, mx, reasons = [], [], set()
@@ -106,7 +124,8 @@ class ClockSampler:
                 if val.lower() == "active":
                     reasons.add(name)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "error": self.error or (self.lines[:1] or [None])[0]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
                 "reasons": sorted(reasons), "samples": len(sm)}
 
