@@ -34,11 +34,12 @@ struct AstroArrays {
     const double* Ca_tot;
     const double* IP3_0;
     const double* tau;
+    const double* inv_tau;  // correctly rounded 1/tau_IP3 per cell (host-formed)
     const double* delta;
 };
 
 struct UniformParams {
-    double Ca_tot, IP3_0, tau, delta;
+    double Ca_tot, IP3_0, tau, delta, inv_tau;
 };
 
 enum InputMode { kInputArray = 0, kInputBernoulli = 1 };
@@ -80,9 +81,11 @@ __device__ __forceinline__ void advance_cell(const StepArgs& a, const AstroArray
                     : a.shared_noise;
     }
     if (kUniform) {
-        astro_rk4(a.k, a.u.Ca_tot, a.u.IP3_0, a.u.tau, a.u.delta, in, noise, ca, ip3, hh);
+        astro_rk4(a.k, a.u.Ca_tot, a.u.IP3_0, a.u.tau, a.u.inv_tau, a.u.delta, in, noise, ca, ip3,
+                  hh);
     } else {
-        astro_rk4(a.k, s.Ca_tot[i], s.IP3_0[i], s.tau[i], s.delta[i], in, noise, ca, ip3, hh);
+        astro_rk4(a.k, s.Ca_tot[i], s.IP3_0[i], s.tau[i], s.inv_tau[i], s.delta[i], in, noise, ca,
+                  ip3, hh);
     }
 }
 
@@ -171,6 +174,7 @@ AstroK make_astro_k(const double* c, double h_step, int substeps) {
     k.Kd_IP3_2 = c[1];
     k.Kd_act = c[2];
     k.ratio_ER_cyt = c[9];
+    k.inv_ratio = 1.0 / c[9];
     k.chan = c[9] * c[6];
     k.serca = c[8];
     k.km2 = c[4] * c[4];
@@ -192,7 +196,7 @@ struct AstroEngine {
     int sms = 148;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    DevBuf Ca, IP3, h, input, Ca_tot, IP3_0, tau, delta, step_base;
+    DevBuf Ca, IP3, h, input, Ca_tot, IP3_0, tau, inv_tau, delta, step_base;
     double last_ms = 0.0;
     std::int64_t last_kernels = 0;
     int shape = 0;  // launch shape (see kShapes), set by asg_astro_autotune
@@ -217,9 +221,9 @@ struct AstroEngine {
     }
 
     AstroArrays arrays() {
-        return AstroArrays{Ca.as<double>(),        IP3.as<double>(),       h.as<double>(),
-                           input.as<double>(),     Ca_tot.as<double>(),    IP3_0.as<double>(),
-                           tau.as<double>(),       delta.as<double>()};
+        return AstroArrays{Ca.as<double>(),     IP3.as<double>(),    h.as<double>(),
+                           input.as<double>(),  Ca_tot.as<double>(), IP3_0.as<double>(),
+                           tau.as<double>(),    inv_tau.as<double>(), delta.as<double>()};
     }
 };
 
@@ -263,6 +267,11 @@ int asg_astro_create(uint32_t n, const double* Ca, const double* IP3, const doub
     upload(e->Ca_tot, Ca_tot, false);
     upload(e->IP3_0, IP3_0, false);
     upload(e->tau, tau_IP3, false);
+    if (tau_IP3 != nullptr) {
+        std::vector<double> inv(n);
+        for (uint32_t i = 0; i < n; ++i) inv[i] = 1.0 / tau_IP3[i];
+        upload(e->inv_tau, inv.data(), false);
+    }
     upload(e->delta, delta_IP3, false);
     if (st == ASG_OK) st = e->step_base.alloc(sizeof(std::int64_t));
     if (st == ASG_OK) {
@@ -382,7 +391,7 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
     std::memset(&a, 0, sizeof a);
     a.n = e->n;
     a.k = asg::make_astro_k(consts, h_step, substeps);
-    a.u = asg::UniformParams{Ca_tot, IP3_0, tau_IP3, delta_IP3};
+    a.u = asg::UniformParams{Ca_tot, IP3_0, tau_IP3, delta_IP3, 1.0 / tau_IP3};
     a.seed = seed;
     a.p = p;
     a.weight = weight;
@@ -485,7 +494,7 @@ extern "C" int asg_astro_autotune(asg_astro* s, const double* consts, double h_s
     a.n = e->n;
     a.k = asg::make_astro_k(consts, h_step, substeps);
     a.u = asg::UniformParams{1.8958264782990153, 0.010925583871830699, 1058.7589568400845,
-                             0.04911592657233997};
+                             0.04911592657233997, 1.0 / 1058.7589568400845};
     a.seed = 1;
     a.p = 0.01;
     a.weight = 0.2;

@@ -108,12 +108,29 @@ struct Draws {
     }
 };
 
+// ------------------------------------------------------------- division
+
+// a / b for a divisor known in advance, from y = RN(1/b) formed once on the
+// host (IEEE division, correctly rounded): q = RN(a*y), r = a - q*b exactly
+// (one FMA), result RN(q + r*y).  Markstein's theorem (P. Markstein, "Computation
+// of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990; Muller et al., Handbook of Floating-Point Arithmetic, on
+// division with a fused multiply-add) guarantees the result equals the
+// correctly rounded a / b whenever y is the correctly rounded reciprocal and
+// no underflow or overflow occurs, i.e. it is bitwise the IEEE quotient the
+// reference computes, in three dependent operations instead of a full divide.
+__device__ __forceinline__ double div_by(double a, double b, double y) {
+    const double q = a * y;
+    const double r = fma(-q, b, a);
+    return fma(r, y, q);
+}
+
 // ------------------------------------------------------ Li-Rinzel astrocyte
 
 // Population constants, with the run-time constant products of the
 // reference's right-hand side pre-formed (same rounding).
 struct AstroK {
-    double Kd_IP3_1, Kd_IP3_2, Kd_act, ratio_ER_cyt;
+    double Kd_IP3_1, Kd_IP3_2, Kd_act, ratio_ER_cyt, inv_ratio;  // inv_ratio = 1/ratio_ER_cyt
     double chan;    // ratio_ER_cyt * rate_IP3R
     double serca;   // rate_SERCA
     double km2;     // Km_SERCA * Km_SERCA
@@ -131,10 +148,12 @@ struct AstroRates {
 };
 
 // d/dt of (Ca, IP3, h) for one cell.
+// `tau` and `inv_tau` (its correctly rounded reciprocal) give dIP3 with
+// div_by; the result is the IEEE quotient (IP3_0 - IP3) / tau.
 __device__ __forceinline__ AstroRates li_rinzel(const AstroK& k, double ca_tot, double ip3_0,
-                                                double tau, double ca, double ip3, double hh,
-                                                double noise) {
-    const double er = (ca_tot - ca) / k.ratio_ER_cyt;  // ER calcium
+                                                double tau, double inv_tau, double ca, double ip3,
+                                                double hh, double noise) {
+    const double er = div_by(ca_tot - ca, k.ratio_ER_cyt, k.inv_ratio);  // ER calcium
     const double ip3_k1 = ip3 + k.Kd_IP3_1;
     const double m = ip3 / ip3_k1;                      // IP3 activation
     const double n = ca / (ca + k.Kd_act);              // Ca activation
@@ -150,27 +169,48 @@ __device__ __forceinline__ AstroRates li_rinzel(const AstroK& k, double ca_tot, 
     const double close_rate = k.k_IP3R * ca;
     AstroRates r;
     r.Ca = release - uptake + leak + noise;
-    r.IP3 = (ip3_0 - ip3) / tau;
+    r.IP3 = div_by(ip3_0 - ip3, tau, inv_tau);
     r.h = open_rate * (1.0 - hh) - close_rate * hh;
     return r;
 }
 
 // Input jump, then `substeps` classical RK4 steps with the physical clamps.
+// kUnroll = false runs the four stages as a loop (one copy of the right-hand
+// side in the instruction stream, for kernels that also hold other roles'
+// code); the weighted stage sum is accumulated left to right either way, so
+// both forms perform the same IEEE operations in the same order.
+template <bool kUnroll = true>
 __device__ __forceinline__ void astro_rk4(const AstroK& k, double ca_tot, double ip3_0, double tau,
-                                          double delta, double input, double noise, double& ca,
-                                          double& ip3, double& hh) {
+                                          double inv_tau, double delta, double input, double noise,
+                                          double& ca, double& ip3, double& hh) {
     if (input != 0.0) ip3 += delta * input;
     for (int s = 0; s < k.substeps; ++s) {
-        const AstroRates a = li_rinzel(k, ca_tot, ip3_0, tau, ca, ip3, hh, noise);
-        const AstroRates b = li_rinzel(k, ca_tot, ip3_0, tau, ca + k.half_h * a.Ca,
-                                       ip3 + k.half_h * a.IP3, hh + k.half_h * a.h, noise);
-        const AstroRates c = li_rinzel(k, ca_tot, ip3_0, tau, ca + k.half_h * b.Ca,
-                                       ip3 + k.half_h * b.IP3, hh + k.half_h * b.h, noise);
-        const AstroRates d = li_rinzel(k, ca_tot, ip3_0, tau, ca + k.h * c.Ca, ip3 + k.h * c.IP3,
-                                       hh + k.h * c.h, noise);
-        ca += k.h6 * (a.Ca + 2.0 * b.Ca + 2.0 * c.Ca + d.Ca);
-        ip3 += k.h6 * (a.IP3 + 2.0 * b.IP3 + 2.0 * c.IP3 + d.IP3);
-        hh += k.h6 * (a.h + 2.0 * b.h + 2.0 * c.h + d.h);
+        double sCa = 0.0, sIP3 = 0.0, sh = 0.0;  // k1 + 2 k2 + 2 k3 + k4, in that order
+        double xCa = ca, xIP3 = ip3, xh = hh;     // stage inputs
+#pragma unroll(kUnroll ? 4 : 1)
+        for (int st = 0; st < 4; ++st) {
+            const AstroRates r = li_rinzel(k, ca_tot, ip3_0, tau, inv_tau, xCa, xIP3, xh, noise);
+            if (st == 0) {
+                sCa = r.Ca;
+                sIP3 = r.IP3;
+                sh = r.h;
+            } else if (st < 3) {
+                sCa = sCa + 2.0 * r.Ca;
+                sIP3 = sIP3 + 2.0 * r.IP3;
+                sh = sh + 2.0 * r.h;
+            } else {
+                sCa = sCa + r.Ca;
+                sIP3 = sIP3 + r.IP3;
+                sh = sh + r.h;
+            }
+            const double step = st < 2 ? k.half_h : k.h;
+            xCa = ca + step * r.Ca;
+            xIP3 = ip3 + step * r.IP3;
+            xh = hh + step * r.h;
+        }
+        ca += k.h6 * sCa;
+        ip3 += k.h6 * sIP3;
+        hh += k.h6 * sh;
         ca = ca < 0.0 ? 0.0 : (ca > ca_tot ? ca_tot : ca);
         hh = hh < 0.0 ? 0.0 : (hh > 1.0 ? 1.0 : hh);
         ip3 = ip3 < 0.0 ? 0.0 : ip3;
@@ -182,6 +222,7 @@ __device__ __forceinline__ void astro_rk4(const AstroK& k, double ca_tot, double
 // Population constants of one neuron population.
 struct NeuronK {
     double C_m, g_L, E_L, V_th, Delta_T, a, tau_w, V_peak, E_ex, E_in, I_e;
+    double inv_C_m, inv_Delta_T, inv_tau_w;  // correctly rounded reciprocals (div_by)
     double neg_g_L;      // -g_L
     double gl_dt;        // g_L * Delta_T
     double psc_ex, psc_in;           // e / tau_syn (neuron.cpp:157-158)
@@ -207,14 +248,15 @@ __device__ __forceinline__ AdexRates adex(const NeuronK& p, double V, double w, 
     const double rel = v - p.E_L;
     AdexRates r;
     if (with_spike) {
-        const double spike = p.gl_dt * exp((v - p.V_th) / p.Delta_T);
+        const double spike = p.gl_dt * exp(div_by(v - p.V_th, p.Delta_T, p.inv_Delta_T));
         const double syn_ex = g_ex * (v - p.E_ex);
         const double syn_in = g_in * (v - p.E_in);
-        r.V = (p.neg_g_L * rel + spike - syn_ex - syn_in - w + p.I_e + I_ext) / p.C_m;
+        r.V = div_by(p.neg_g_L * rel + spike - syn_ex - syn_in - w + p.I_e + I_ext, p.C_m,
+                     p.inv_C_m);
     } else {
         r.V = 0.0;
     }
-    r.w = (p.a * rel - w) / p.tau_w;
+    r.w = div_by(p.a * rel - w, p.tau_w, p.inv_tau_w);
     return r;
 }
 

@@ -32,6 +32,9 @@ NeuronK make_neuron_k(const asg_neuron_params& p, const asg_input& in, double dt
     k.E_ex = p.E_ex;
     k.E_in = p.E_in;
     k.I_e = p.I_e;
+    k.inv_C_m = 1.0 / p.C_m;
+    k.inv_Delta_T = 1.0 / p.Delta_T;
+    k.inv_tau_w = 1.0 / p.tau_w;
     k.neg_g_L = -p.g_L;
     k.gl_dt = p.g_L * p.Delta_T;
     k.psc_ex = kE / p.tau_syn_ex;
@@ -55,6 +58,7 @@ AstroK make_astro_k(const asg_astro_params& a, double h, int substeps) {
     k.Kd_IP3_2 = a.Kd_IP3_2;
     k.Kd_act = a.Kd_act;
     k.ratio_ER_cyt = a.ratio_ER_cyt;
+    k.inv_ratio = 1.0 / a.ratio_ER_cyt;
     k.chan = a.ratio_ER_cyt * a.rate_IP3R;
     k.serca = a.rate_SERCA;
     k.km2 = a.Km_SERCA * a.Km_SERCA;
@@ -351,6 +355,8 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     D.U = d.stp.U;
     D.tau_rec = d.stp.tau_rec;
     D.tau_fac = d.stp.tau_fac;
+    D.inv_tau_rec = 1.0 / d.stp.tau_rec;
+    D.inv_tau_fac = d.stp.tau_fac > 0.0 ? 1.0 / d.stp.tau_fac : 0.0;
 
     // Per-cell astrocyte parameters collapse to scalars when all equal.
     const double* pa[4] = {d.Ca_tot, d.IP3_0, d.tau_IP3, d.delta_IP3};
@@ -374,6 +380,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     D.IP3_0_u = uval[1];
     D.tau_u = uval[2];
     D.delta_u = uval[3];
+    D.inv_tau_u = 1.0 / uval[2];
 
     // Host preprocessing of the tables.
     static const std::uint32_t zero_rs[1] = {0};
@@ -429,10 +436,14 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     add_seg(D.Ca, a8, d.Ca ? d.Ca : Ca0.data());
     add_seg(D.IP3, a8, d.IP3 ? d.IP3 : IP30.data());
     add_seg(D.h, a8, d.h ? d.h : h0.data());
+    std::vector<double> inv_tau;
     if (!uniform) {
+        inv_tau.resize(NA);
+        for (std::uint32_t i = 0; i < NA; ++i) inv_tau[i] = 1.0 / d.tau_IP3[i];
         add_seg(D.Ca_tot, a8, d.Ca_tot);
         add_seg(D.IP3_0, a8, d.IP3_0);
         add_seg(D.tau, a8, d.tau_IP3);
+        add_seg(D.inv_tau, a8, inv_tau.data());
         add_seg(D.delta, a8, d.delta_IP3);
     }
     add_seg(D.stp_x, n8, stp_x.data());

@@ -85,7 +85,7 @@ struct InstDev {
     // astrocytes
     AstroK ak;
     std::int32_t astro_uniform;
-    double Ca_tot_u, IP3_0_u, tau_u, delta_u;
+    double Ca_tot_u, IP3_0_u, tau_u, delta_u, inv_tau_u;
     double a_rate, a_weight, a_lambda, a_limit, a_std;
     std::int32_t a_indep, a_steps_per_noise;
     double SIC_scale, SIC_th;
@@ -97,7 +97,8 @@ struct InstDev {
     const double *V_reset, *b;
     // astrocyte state / params
     double *Ca, *IP3, *h;
-    const double *Ca_tot, *IP3_0, *tau, *delta;
+    const double *Ca_tot, *IP3_0, *tau, *inv_tau, *delta;
+    double inv_tau_rec, inv_tau_fac;  // correctly rounded reciprocals (div_by)
     // STP per source
     double *stp_x, *stp_u, *stp_t;
     // out-edge CSR (source order) of the three spike-carrying sets

@@ -231,15 +231,32 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
                 const AdexRates r = adex<false>(P, V, w, gex, gin, Iext);
                 w += h * r.w;
             } else {
+                // RK4 with the conductances at the start, midpoint and end of
+                // the substep (neuron.cpp:285-298), stages as a loop; the stage
+                // sum k1 + 2 k2 + 2 k3 + k4 accumulates left to right.
                 const double gexm = 0.5 * (gex + gex1), ginm = 0.5 * (gin + gin1);
-                const AdexRates k1 = adex<true>(P, V, w, gex, gin, Iext);
-                const AdexRates k2 =
-                    adex<true>(P, V + half_h * k1.V, w + half_h * k1.w, gexm, ginm, Iext);
-                const AdexRates k3 =
-                    adex<true>(P, V + half_h * k2.V, w + half_h * k2.w, gexm, ginm, Iext);
-                const AdexRates k4 = adex<true>(P, V + h * k3.V, w + h * k3.w, gex1, gin1, Iext);
-                V += h6 * (k1.V + 2.0 * k2.V + 2.0 * k3.V + k4.V);
-                w += h6 * (k1.w + 2.0 * k2.w + 2.0 * k3.w + k4.w);
+                double sV = 0.0, sw = 0.0, xV = V, xw = w;
+#pragma unroll 1
+                for (int st = 0; st < 4; ++st) {
+                    const double ge = st == 0 ? gex : (st < 3 ? gexm : gex1);
+                    const double gi = st == 0 ? gin : (st < 3 ? ginm : gin1);
+                    const AdexRates r = adex<true>(P, xV, xw, ge, gi, Iext);
+                    if (st == 0) {
+                        sV = r.V;
+                        sw = r.w;
+                    } else if (st < 3) {
+                        sV = sV + 2.0 * r.V;
+                        sw = sw + 2.0 * r.w;
+                    } else {
+                        sV = sV + r.V;
+                        sw = sw + r.w;
+                    }
+                    const double stp = st < 2 ? half_h : h;
+                    xV = V + stp * r.V;
+                    xw = w + stp * r.w;
+                }
+                V += h6 * sV;
+                w += h6 * sw;
             }
             gex = gex1;
             dgex = dgex1;
@@ -269,8 +286,9 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
             if (I.stp_on) {
                 const double t_now = static_cast<double>(step) * I.dt;
                 const double d = t_now - I.stp_t[c];
-                const double xd = exp(-d / I.tau_rec);
-                const double ud = I.tau_fac < 1e-10 ? 0.0 : exp(-d / I.tau_fac);
+                const double xd = exp(div_by(-d, I.tau_rec, I.inv_tau_rec));
+                const double ud =
+                    I.tau_fac < 1e-10 ? 0.0 : exp(div_by(-d, I.tau_fac, I.inv_tau_fac));
                 x = I.stp_x[c];
                 u = I.stp_u[c];
                 x = 1.0 + (x - x * u - 1.0) * xd;
@@ -354,10 +372,11 @@ __device__ void astro_role(const InstDev& I, const Work& wk, std::int64_t step) 
                           : I.a_std * normal_clamped(nseed, idx);
     }
     if (I.astro_uniform) {
-        astro_rk4(I.ak, I.Ca_tot_u, I.IP3_0_u, I.tau_u, I.delta_u, ip3_in, noise, ca, ip3, hh);
+        astro_rk4<false>(I.ak, I.Ca_tot_u, I.IP3_0_u, I.tau_u, I.inv_tau_u, I.delta_u, ip3_in,
+                         noise, ca, ip3, hh);
     } else {
-        astro_rk4(I.ak, I.Ca_tot[a], I.IP3_0[a], I.tau[a], I.delta[a], ip3_in, noise, ca, ip3,
-                  hh);
+        astro_rk4<false>(I.ak, I.Ca_tot[a], I.IP3_0[a], I.tau[a], I.inv_tau[a], I.delta[a],
+                         ip3_in, noise, ca, ip3, hh);
     }
     I.Ca[a] = ca;
     I.IP3[a] = ip3;

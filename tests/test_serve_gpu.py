@@ -22,14 +22,14 @@ def alone(model, steps):
 
 
 def test_requests_same_alone_and_in_mix():
-    specs = [("quick", 1, 900), ("use_case", 2, 1500), ("quick", 3, 400), ("bursting", 4, 1200),
-             ("use_case", 5, 700)]
+    specs = [("quick", 1, 9000), ("use_case", 2, 15000), ("quick", 3, 4000),
+             ("bursting", 4, 12000), ("use_case", 5, 7000)]
     models = [Model(config_path(n), seed=s, pre_time=0.0) for n, s, _ in specs]
     srv = Server(chunk_steps=64)
     ids = []
     for m, (_, _, steps) in zip(models, specs):
         ids.append(srv.submit(m, steps))
-        time.sleep(0.01)  # staggered arrivals: later ones join a running batch
+        time.sleep(0.02)  # staggered arrivals: later ones join a running batch
     res = [srv.wait(i, 60000.0) for i in ids]
     assert all(r.status == 0 for r in res)
     for i, (m, (_, _, steps)) in enumerate(zip(models, specs)):
