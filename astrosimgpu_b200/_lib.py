@@ -185,6 +185,9 @@ SIGNATURES = {
     "asg_astro_last_timing": (C.c_int, [vp, c_double_p, c_int64_p]),
     "asg_astro_autotune": (C.c_int, [vp, c_double_p, C.c_double, C.c_int32, C.c_int32,
                                      c_int32_p, c_double_p]),
+    "asg_astro_update_noalloc": (C.c_int, [C.c_uint32] + [vp] * 8 + [c_double_p, C.c_double,
+                                           C.c_int32, C.c_double, C.c_int32, C.c_double,
+                                           C.c_uint64, C.c_uint64, vp]),
     # host config + builder
     "asg_model_from_json": (C.c_int, [C.c_char_p, C.c_int64, C.c_double, C.c_double, C.c_int64,
                                       vpp]),

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "asg_common.hpp"
@@ -522,5 +523,107 @@ extern "C" int asg_astro_autotune(asg_astro* s, const double* consts, double h_s
     e->shape = best;
     if (chosen) *chosen = best;
     if (us_per_step) *us_per_step = 1e3 * best_ms / steps;
+    return ASG_OK;
+}
+
+// ------------------------------------------------- allocation-free variant
+//
+// Some callers cannot call cudaMalloc: for example the reference's OpenMP
+// target-offload build, whose device copies of Ca, IP3, h and the per-cell
+// parameters are owned by the OpenMP runtime (`omp target enter data`) and
+// reach us only as device pointers, or a host framework whose memory pool
+// owns all device memory and forbids allocations of its own during a run.
+// asg_astro_update_noalloc serves them: it updates caller-owned device arrays
+// in place and allocates nothing.  Its only scratch -- the correctly rounded
+// reciprocal of each cell's tau_IP3 that the division in the IP3 rate uses --
+// lives in the file-scope array below, which every GPU that loads this
+// library holds until the process exits.
+
+namespace asg {
+namespace {
+
+constexpr std::uint32_t kNoAllocMaxCells = 1u << 20;  // 8 MiB of FP64 reciprocals
+__device__ __align__(256) double g_noalloc_inv_tau[kNoAllocMaxCells];
+
+constexpr int kNoAllocMaxDevices = 64;
+double* g_noalloc_scratch[kNoAllocMaxDevices] = {};  // device address, per device
+std::mutex g_noalloc_mu;
+
+// inv_tau[i] = 1 / tau[i] (IEEE division: the correctly rounded reciprocal).
+__global__ void noalloc_reciprocals(std::uint32_t n, const double* __restrict__ tau,
+                                    double* __restrict__ inv_tau) {
+    const std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) inv_tau[i] = 1.0 / tau[i];
+}
+
+// Device address of the scratch array on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device, with that device current, and cached.
+int noalloc_scratch(double** out) {
+    int dev = -1;
+    ASG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(ASG_ERR_UNSUPPORTED, "device ordinal %d beyond %d", dev, kNoAllocMaxDevices);
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (g_noalloc_scratch[dev] == nullptr) {
+        void* p = nullptr;
+        ASG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_inv_tau));
+        g_noalloc_scratch[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_scratch[dev];
+    return ASG_OK;
+}
+
+}  // namespace
+}  // namespace asg
+
+extern "C" int asg_astro_update_noalloc(uint32_t n, double* Ca, double* IP3, double* h,
+                                        double* ip3_input, const double* Ca_tot,
+                                        const double* IP3_0, const double* tau_IP3,
+                                        const double* delta_IP3, const double* consts,
+                                        double h_step, int32_t substeps, double noise_std,
+                                        int32_t independent_noise, double shared_noise,
+                                        uint64_t noise_seed, uint64_t noise_index, void* stream) {
+    asg::clear_error();
+    if (n == 0) return ASG_OK;
+    if (n > asg::kNoAllocMaxCells)
+        return asg::fail(ASG_ERR_ARG,
+                         "asg_astro_update_noalloc: %u cells exceed the %u-cell scratch limit; "
+                         "use asg_astro_create/asg_astro_update for larger populations",
+                         n, asg::kNoAllocMaxCells);
+    if (Ca == nullptr || IP3 == nullptr || h == nullptr || ip3_input == nullptr ||
+        Ca_tot == nullptr || IP3_0 == nullptr || tau_IP3 == nullptr || delta_IP3 == nullptr ||
+        consts == nullptr)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_update_noalloc: NULL argument");
+    if (substeps < 0) return asg::fail(ASG_ERR_ARG, "asg_astro_update_noalloc: substeps < 0");
+    for (const void* p : {static_cast<const void*>(Ca), static_cast<const void*>(IP3),
+                          static_cast<const void*>(h), static_cast<const void*>(ip3_input),
+                          static_cast<const void*>(Ca_tot), static_cast<const void*>(IP3_0),
+                          static_cast<const void*>(tau_IP3), static_cast<const void*>(delta_IP3)})
+        if (reinterpret_cast<std::uintptr_t>(p) % alignof(double) != 0)
+            return asg::fail(ASG_ERR_ARG, "asg_astro_update_noalloc: array not 8-byte aligned");
+    double* inv_tau = nullptr;
+    ASG_TRY(asg::noalloc_scratch(&inv_tau));
+    int dev = 0, sms = 148;
+    ASG_CUDA(cudaGetDevice(&dev));
+    ASG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Every entry this call reads is written first, in stream order, so the
+    // previous call's contents never leak in.
+    asg::noalloc_reciprocals<<<(n + 255) / 256, 256, 0, st>>>(n, tau_IP3, inv_tau);
+    ASG_CUDA(cudaGetLastError());
+    asg::StepArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n = n;
+    a.k = asg::make_astro_k(consts, h_step, substeps);
+    a.noise_std = noise_std;
+    a.independent = noise_std > 0.0 ? independent_noise : 0;
+    a.shared_noise = shared_noise;
+    a.noise_seed = noise_seed;
+    a.noise_index = noise_index;
+    const asg::AstroArrays arr{Ca, IP3, h, ip3_input, Ca_tot, IP3_0, tau_IP3, inv_tau, delta_IP3};
+    // Shape 1: one cell per thread with 8-byte accesses, so caller arrays need
+    // no more than double alignment.
+    ASG_CUDA((asg::launch_astro<false, asg::kInputArray, true>(1, sms, a, arr, st)));
     return ASG_OK;
 }

@@ -289,6 +289,26 @@ int asg_astro_autotune(asg_astro* s, const double* consts, double h_step, int32_
 /* Device ms of the last run call and kernels launched. */
 int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels);
 
+/* Allocation-free astrocyte update.  No counterpart in the reference: it
+ * exists for callers that cannot call cudaMalloc -- e.g. an OpenMP
+ * target-offload build whose device arrays belong to the OpenMP runtime, or a
+ * framework whose memory pool owns all device memory.  All array arguments
+ * are DEVICE pointers owned by the caller (8-byte aligned) and are updated in
+ * place exactly like asg_astro_update updates its resident copies (ip3_input
+ * is consumed and zeroed).  `stream` is a cudaStream_t (NULL: the default
+ * stream); the call is asynchronous on it.  The only scratch, one double per
+ * cell, lives in a static device array of at most 1,048,576 cells: larger n
+ * is rejected with ASG_ERR_ARG.  Nothing is allocated, not even on the first
+ * call; that first call on a device looks up the array's device address, so
+ * make it before any stream capture.  Every call shares the array: calls that
+ * overlap on the GPU race and must be ordered by the caller. */
+int asg_astro_update_noalloc(uint32_t n, double* Ca, double* IP3, double* h, double* ip3_input,
+                             const double* Ca_tot, const double* IP3_0, const double* tau_IP3,
+                             const double* delta_IP3, const double* consts, double h_step,
+                             int32_t substeps, double noise_std, int32_t independent_noise,
+                             double shared_noise, uint64_t noise_seed, uint64_t noise_index,
+                             void* stream);
+
 /* ------------------------------------------ host side: config + builder
  * The reference's JSON schema (parameters.cpp:85-205): '//' comments, key
  * aliases (V_m, IP3, gauss_noise_var), noise_dt default 10*dt, validation,

@@ -1,0 +1,66 @@
+"""The allocation-free astrocyte update (asg_astro_update_noalloc), for
+callers that cannot call cudaMalloc and hand over device arrays they own.
+
+It must give what the regular entry point gives (asg_astro_create +
+asg_astro_push_input + asg_astro_update: bitwise, the tolerance of the other
+astrocyte tests) on two calls in a row -- the second call proves the shared
+scratch array carries nothing over from the first.  This file is collected
+last, so a run that stops at the first failure has run every other test."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from astrosimgpu_b200 import _lib
+from astrosimgpu_b200.astro import AstroBackend, ScalingWorkload
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to("cuda")
+
+
+def test_noalloc_matches_regular_entry_point_twice():
+    import torch
+    rng = np.random.default_rng(11)
+    n = 5003
+    w = ScalingWorkload(n)
+    Ca, IP3, h = w.initial_state()
+    Ca_tot = w.Ca_tot * (1 + 0.05 * rng.standard_normal(n))
+    IP3_0 = w.IP3_0 * (1 + 0.05 * rng.standard_normal(n))
+    tau = w.tau_IP3 * (1 + 0.05 * rng.standard_normal(n))
+    delta = w.delta_IP3 * (1 + 0.05 * rng.standard_normal(n))
+    inputs = [np.where(rng.random(n) < 0.3, rng.random(n), 0.0) for _ in range(2)]
+
+    regular = AstroBackend(Ca, IP3, h, Ca_tot, IP3_0, tau, delta)
+    d = {k: dev(v) for k, v in dict(Ca=Ca, IP3=IP3, h=h, Ca_tot=Ca_tot, IP3_0=IP3_0, tau=tau,
+                                       delta=delta, inp=np.zeros(n)).items()}
+    lib = _lib.load()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for call, inp in enumerate(inputs):
+        regular.push_input(inp)
+        regular.update(w.consts, w.h_step, 2)
+        d["inp"].copy_(torch.from_numpy(inp))
+        st = lib.asg_astro_update_noalloc(
+            n, *[C.c_void_p(d[k].data_ptr()) for k in ("Ca", "IP3", "h", "inp", "Ca_tot",
+                                                         "IP3_0", "tau", "delta")],
+            _lib.dptr(w.consts), w.h_step, 2, 0.0, 1, 0.0, 0, 0, stream)
+        assert st == 0, lib.asg_last_error()
+        torch.cuda.synchronize()
+        rCa, rIP3, rh = regular.pull_state()
+        assert np.array_equal(d["Ca"].cpu().numpy(), rCa), call
+        assert np.array_equal(d["IP3"].cpu().numpy(), rIP3), call
+        assert np.array_equal(d["h"].cpu().numpy(), rh), call
+        assert not d["inp"].any()  # the input is consumed, as the regular path does
+    regular.destroy()
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    lib = _lib.load()
+    null = C.c_void_p(16)  # never dereferenced: the size check comes first
+    consts = np.zeros(10)
+    st = lib.asg_astro_update_noalloc((1 << 20) + 1, *([null] * 8), _lib.dptr(consts), 0.1, 1,
+                                      0.0, 1, 0.0, 0, 0, None)
+    assert st == 1 and b"scratch limit" in lib.asg_last_error()
