@@ -107,7 +107,7 @@ class State(C.Structure):
 class EngineOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("chunk_steps", C.c_int32), ("block", C.c_int32),
                 ("use_graphs", C.c_int32), ("sic_mode", C.c_int32), ("pdl", C.c_int32),
-                ("mem_budget", C.c_uint64)]
+                ("push_mode", C.c_int32), ("mem_budget", C.c_uint64)]
 
 
 class ServeOpts(C.Structure):
@@ -200,6 +200,7 @@ SIGNATURES = {
     "asg_model_scalars": (C.c_int, [vp, c_double_p]),
     "asg_model_stats": (C.c_int, [vp, c_int64_p]),
     "asg_model_free": (C.c_int, [vp]),
+    "asg_selftest_barrier_timeout": (C.c_int, [c_int32_p, c_double_p]),
     "asg_calcium_analysis": (C.c_int, [c_double_p, c_double_p, C.c_int32, C.c_int32, C.c_double,
                                        C.c_double, C.c_double, C.c_double, C.c_double,
                                        C.c_double, c_double_p]),

@@ -17,9 +17,10 @@ EngineConfig config_from(const asg_engine_opts* o) {
         c.device = o->device;
         if (o->chunk_steps > 0) c.chunk_steps = o->chunk_steps;
         if (o->block > 0) c.block = o->block;
-        if (o->use_graphs != 0) c.use_graphs = o->use_graphs;
+        if (o->use_graphs != 0) c.use_graphs = o->use_graphs;  // -1 plain, 2 persistent
         c.sic_mode = o->sic_mode;
         c.pdl = o->pdl >= 0;
+        c.push_mode = o->push_mode;
         c.mem_budget = o->mem_budget;
     }
     return c;
@@ -388,6 +389,8 @@ int asg_batch_autotune(asg_batch* b, int32_t steps, asg_engine_opts* chosen) {
         chosen->block = best_block;
         chosen->use_graphs = e.cfg.use_graphs;
         chosen->sic_mode = e.cfg.sic_mode;
+        chosen->pdl = e.cfg.pdl ? 0 : -1;
+        chosen->push_mode = e.cfg.push_mode;
         chosen->mem_budget = e.cfg.mem_budget;
     }
     (void)block0;
@@ -401,3 +404,26 @@ int asg_batch_destroy(asg_batch* b) {
 }
 
 }  // extern "C"
+
+extern "C" int asg_selftest_barrier_timeout(int32_t* timed_out, double* wait_ms) {
+    asg::clear_error();
+    if (timed_out == nullptr) return asg::fail(ASG_ERR_ARG, "asg_selftest_barrier_timeout: NULL");
+    asg::DevBuf gb;
+    ASG_TRY(gb.alloc(sizeof(asg::GridBarrier)));
+    cudaEvent_t a, b;
+    ASG_CUDA(cudaEventCreate(&a));
+    ASG_CUDA(cudaEventCreate(&b));
+    ASG_CUDA(cudaEventRecord(a, nullptr));
+    ASG_CUDA(asg::barrier_selftest(gb.as<asg::GridBarrier>(), nullptr));
+    ASG_CUDA(cudaEventRecord(b, nullptr));
+    ASG_CUDA(cudaEventSynchronize(b));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    asg::GridBarrier h{};
+    ASG_CUDA(cudaMemcpy(&h, gb.get(), sizeof h, cudaMemcpyDeviceToHost));
+    *timed_out = h.error != 0;
+    if (wait_ms) *wait_ms = ms;
+    return ASG_OK;
+}

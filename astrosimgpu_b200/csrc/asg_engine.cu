@@ -225,6 +225,7 @@ Engine::~Engine() {
     for (int p = 0; p < 2; ++p) {
         if (h_insts[p]) cudaFreeHost(h_insts[p]);
         if (h_stats[p]) cudaFreeHost(h_stats[p]);
+        if (h_barrier_err[p]) cudaFreeHost(h_barrier_err[p]);
         if (ev_chunk[p]) cudaEventDestroy(ev_chunk[p]);
         if (ev_chunk0[p]) cudaEventDestroy(ev_chunk0[p]);
     }
@@ -257,7 +258,10 @@ int Engine::init() {
     for (int p = 0; p < 2; ++p) {
         ASG_CUDA(cudaEventCreate(&ev_chunk[p]));
         ASG_CUDA(cudaEventCreate(&ev_chunk0[p]));
+        ASG_CUDA(cudaHostAlloc(&h_barrier_err[p], sizeof(unsigned), cudaHostAllocDefault));
+        *h_barrier_err[p] = 0;
     }
+    ASG_TRY(d_barrier.alloc(sizeof(GridBarrier)));
     return ASG_OK;
 }
 
@@ -332,6 +336,11 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     D.fused_sic = cfg.sic_mode == 1 ? 1 : cfg.sic_mode == 2 ? (D.d_a2n >= 2 ? 0 : 1)
                                                             : (D.d_a2n >= 2 ? 0 : 1);
     D.stp_on = d.stp.enabled != 0;
+    // Deferred push needs both spike delays >= 2 steps (the push of step s
+    // runs in step s+1 and must land before step s+d reads it).
+    D.deferred_push = (cfg.push_mode != 1 && d.d_e_steps >= 2 && d.d_i_steps >= 2) ? 1 : 0;
+    D.push_blocks = static_cast<std::int32_t>(
+        std::min<std::uint32_t>(128, std::max<std::uint32_t>(1, (N + 255) / 256)));
     D.seed = d.seed;
     D.dt = d.dt;
     const double h = d.dt / static_cast<double>(d.substeps);
@@ -470,6 +479,9 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     ring_segs(D.ring_in, rin, N);
     ring_segs(D.ring_as, ras, NA);
 
+    add_seg(D.spk_packed, 4 * 8, nullptr);
+    add_seg(D.spk_meta, 3 * std::max<std::size_t>(N, 1) * 16, nullptr);
+    add_seg(D.spk_val, 3 * std::max<std::size_t>(N, 1) * 16, nullptr);
     add_seg(D.sic_soff, sic.soff.size() * 4, sic.soff.data());
     add_seg(D.sic_ent, sic.ent.size() * 4, sic.ent.data());
     add_seg(D.fac, S * std::max<std::size_t>(a8, 8), nullptr);
@@ -586,12 +598,24 @@ int Engine::rebuild() {
     const int B = cfg.block;
     work.clear();
     order.clear();
-    // SIC blocks first (longest dependent chains), then neurons, then astrocytes.
-    for (int role = 0; role < 3; ++role) {
+    // Push and SIC blocks first (longest dependent chains), then neurons, then
+    // astrocytes.  A PUSH item's `first` is its index among the instance's
+    // push blocks.
+    for (int role = 0; role < 4; ++role) {
         for (std::size_t s = 0; s < insts.size(); ++s) {
             const InstDev& D = insts[s]->dev;
-            const std::uint16_t r = role == 0 ? kRoleSic : role == 1 ? kRoleNeuron : kRoleAstro;
+            const std::uint16_t r = role == 0   ? kRolePush
+                                    : role == 1 ? kRoleSic
+                                    : role == 2 ? kRoleNeuron
+                                                : kRoleAstro;
             if (r == kRoleSic && D.fused_sic) continue;
+            if (r == kRolePush) {
+                if (!D.deferred_push) continue;
+                for (int pb = 0; pb < D.push_blocks; ++pb)
+                    work.push_back(Work{static_cast<std::uint32_t>(s), r, 0,
+                                        static_cast<std::uint32_t>(pb), 0});
+                continue;
+            }
             const std::uint32_t n = r == kRoleAstro ? D.NA : D.N;
             for (std::uint32_t f = 0; f < n; f += B)
                 work.push_back(Work{static_cast<std::uint32_t>(s), r, 0, f,
@@ -624,7 +648,13 @@ int Engine::rebuild() {
     ASG_CUDA(cudaMemsetAsync(d_stats.get(), 0, cap_insts * 8 * sizeof(unsigned long long), stream));
     ASG_CUDA(cudaStreamSynchronize(stream));
     graph_steps = 0;
-    if (cfg.use_graphs >= 0 && !work.empty()) {
+    persistent_grid = 0;
+    if (cfg.use_graphs == 2 && !work.empty()) {
+        const int cap = persistent_blocks(B);
+        if (cap <= 0) return fail(ASG_ERR_CUDA, "persistent kernel: no co-resident blocks");
+        persistent_grid = std::min<int>(cap, static_cast<int>(work.size()));
+    }
+    if ((cfg.use_graphs == 0 || cfg.use_graphs == 1) && !work.empty()) {
         cudaGraph_t g = nullptr;
         ASG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t le = cudaSuccess;
@@ -671,15 +701,24 @@ int Engine::launch_chunk(int parity, int steps) {
     ASG_CUDA(cudaEventRecord(ev_chunk0[parity], stream));
     ASG_CUDA(cudaMemcpyAsync(d_insts.get(), hi, insts.size() * sizeof(InstDev),
                              cudaMemcpyHostToDevice, stream));
-    if (graph != nullptr && steps == graph_steps) {
+    if (persistent_grid > 0) {
+        ASG_CUDA(cudaMemsetAsync(d_barrier.get(), 0, sizeof(GridBarrier), stream));
+        ASG_CUDA(launch_chunk_persistent(d_insts.as<InstDev>(), d_work.as<Work>(),
+                                         static_cast<int>(work.size()), cfg.block,
+                                         persistent_grid, steps, d_barrier.as<GridBarrier>(),
+                                         stream));
+        ASG_CUDA(cudaMemcpyAsync(h_barrier_err[parity], &d_barrier.as<GridBarrier>()->error,
+                                 sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    } else if (graph != nullptr && steps == graph_steps) {
         ASG_CUDA(cudaGraphLaunch(graph, stream));
     } else {
         for (int k = 0; k < steps; ++k)
             ASG_CUDA(launch_step(d_insts.as<InstDev>(), d_work.as<Work>(),
                                  static_cast<int>(work.size()), cfg.block, k, cfg.pdl, stream));
     }
-    last_kernels += steps;
-    launched_kernels += steps;
+    const int launched = persistent_grid > 0 ? 1 : steps;
+    last_kernels += launched;
+    launched_kernels += launched;
     ASG_CUDA(cudaMemcpyAsync(h_stats[parity], d_stats.get(),
                              insts.size() * 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              stream));
@@ -699,6 +738,12 @@ int Engine::collect(int parity) {
     float chunk_ms = 0.0f;
     if (cudaEventElapsedTime(&chunk_ms, ev_chunk0[parity], ev_chunk[parity]) == cudaSuccess)
         chunk_device_ms += chunk_ms;
+    if (*h_barrier_err[parity] != 0) {
+        *h_barrier_err[parity] = 0;
+        return fail(ASG_ERR_TIMEOUT,
+                    "persistent step kernel: a grid barrier wait gave up; the chunk's results "
+                    "are invalid");
+    }
     const unsigned long long* st = h_stats[parity];
     const std::size_t n_launched = std::min(insts.size(), launched_insts[parity]);
     for (std::size_t s = 0; s < n_launched; ++s) {

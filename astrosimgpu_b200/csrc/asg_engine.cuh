@@ -47,7 +47,7 @@
 
 namespace asg {
 
-enum Role : std::uint16_t { kRoleNeuron = 0, kRoleAstro = 1, kRoleSic = 2 };
+enum Role : std::uint16_t { kRoleNeuron = 0, kRoleAstro = 1, kRoleSic = 2, kRolePush = 3 };
 
 struct Work {
     std::uint32_t inst;
@@ -104,6 +104,17 @@ struct InstDev {
     // out-edge CSR (source order) of the three spike-carrying sets
     const std::uint32_t *exc_rs, *exc_tg, *inh_rs, *inh_tg, *n2a_rs, *n2a_tg;
     InRing ring_ex, ring_in, ring_as;
+    // Deferred push (both spike delays >= 2 steps): each spike of step s
+    // reserves a contiguous range of that step's flat edge space (one 64-bit
+    // atomic: list index in the high bits, edge offset in the low 40) and is
+    // pushed in step s+1 by the PUSH blocks, whose threads stride over the
+    // flat space -- every edge of every spike gets one thread, whatever the
+    // spike count.  Three list slots rotate: append (s), push (s-1), reset (s+1).
+    std::int32_t deferred_push;
+    std::int32_t push_blocks;          // PUSH work items of this instance
+    unsigned long long* spk_packed;    // [3]: count << 40 | edges
+    std::uint32_t* spk_meta;           // [3][N][4]: source, edge offset, row0 start, row0 length
+    double* spk_val;                   // [3][N][2]: exc or inh set value, n2a value
     // SIC: sliced ELL over targets, factors per emission slot, split values
     const std::uint32_t* sic_soff;  // [n_slices+1] entry offset of each 32-target slice
     const std::uint32_t* sic_ent;   // astro << 8 | mult
@@ -120,6 +131,22 @@ struct InstDev {
     double *rec_Ca, *rec_IP3, *rec_V, *rec_Isic;             // [rec_rows][max]
     unsigned long long* counters;  // spike_edges, sic_edges, spikes, overflow
 };
+
+// Barrier words of the persistent chunk kernel (device memory, zeroed).
+struct GridBarrier {
+    unsigned count, gen, error, pad;
+};
+
+// Launches 4 blocks of which one never reaches the barrier (self-test of the
+// bounded wait: the others must give up and set gb->error).
+cudaError_t barrier_selftest(GridBarrier* gb, cudaStream_t stream);
+
+// Co-resident blocks of the persistent chunk kernel at this block size.
+int persistent_blocks(int block);
+// All `steps` steps of a chunk in one cooperative launch of `grid` blocks.
+cudaError_t launch_chunk_persistent(const InstDev* insts, const Work* work, int n_work,
+                                    int block, int grid, int steps, GridBarrier* gb,
+                                    cudaStream_t stream);
 
 // One step launch; with `pdl` the launch may start while the previous kernel
 // of the stream is still running (the kernel waits for it before any access

@@ -55,9 +55,10 @@ struct EngineConfig {
     int device = 0;
     int chunk_steps = 32;
     int block = 128;
-    int use_graphs = 1;
+    int use_graphs = 1;  // 1 graphs of per-step launches, -1 plain launches, 2 persistent
     int sic_mode = 0;  // 0 auto, 1 fused, 2 split
     bool pdl = true;   // programmatic dependent launch between steps
+    int push_mode = 0; // 0 deferred push when delays allow, 1 always in the spiking block
     std::uint64_t mem_budget = 0;
 };
 
@@ -113,6 +114,9 @@ private:
     InstDev* h_insts[2] = {nullptr, nullptr};  // pinned staging
     unsigned long long* h_stats[2] = {nullptr, nullptr};  // pinned: per inst log_n + counters
     DevBuf d_stats;        // [n][8]: log_n, spike_edges, sic_edges, spikes, overflow
+    DevBuf d_barrier;      // GridBarrier of the persistent chunk kernel
+    unsigned* h_barrier_err[2] = {nullptr, nullptr};  // pinned copy of its error word
+    int persistent_grid = 0;
     std::size_t cap_insts = 0;
     std::vector<Work> work;
     std::vector<int> order;  // instance index per device slot

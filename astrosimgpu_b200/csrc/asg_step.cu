@@ -43,7 +43,7 @@ __device__ __forceinline__ double ring_gather(const InRing& R, int slot, std::ui
     auto flush = [&]() {
         double v[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = k < n ? vals[idx[k]] : 0.0;
+        for (int k = 0; k < 8; ++k) v[k] = k < n ? __ldcg(vals + idx[k]) : 0.0;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             if (k < n) {
@@ -87,7 +87,7 @@ __device__ __forceinline__ double ring_gather(const InRing& R, int slot, std::ui
         }
         if (nq == 0) break;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) wv[k] = k < nq ? bits[q[k]] : 0u;
+        for (int k = 0; k < 8; ++k) wv[k] = k < nq ? __ldcg(bits + q[k]) : 0u;
 #pragma unroll
         for (int k = 0; k < 8; ++k)
             if (k < nq && wv[k] != 0) bits[q[k]] = 0;
@@ -114,7 +114,7 @@ __device__ __forceinline__ double sic_sum(const InstDev& I, std::uint32_t t, int
 #pragma unroll
         for (int k = 0; k < 8; ++k) e[k] = b0 + k < len ? __ldg(I.sic_ent + o0 + (b0 + k) * 32 + lane) : 0u;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) f[k] = (e[k] & 0xFFu) ? fac[e[k] >> 8] : 0.0;
+        for (int k = 0; k < 8; ++k) f[k] = (e[k] & 0xFFu) ? __ldcg(fac + (e[k] >> 8)) : 0.0;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const std::uint32_t m = e[k] & 0xFFu;
@@ -164,11 +164,11 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
         const std::size_t so = static_cast<std::size_t>(slot);
         unsigned long long* sp_ex = I.ring_ex.sum + so * I.ring_ex.n_targets + c;
         unsigned long long* sp_in = I.ring_in.sum + so * I.ring_in.n_targets + c;
-        const unsigned long long g_ex = *sp_ex, g_in = *sp_in;
+        const unsigned long long g_ex = __ldcg(sp_ex), g_in = __ldcg(sp_in);
         const std::int64_t se = step - I.d_a2n;
         const bool sic_due = se >= 0 && se % I.sic_interval == 0;
         double Isic = (sic_due && !I.fused_sic)
-                          ? I.sic_val[static_cast<std::size_t>(step & 1) * I.N + c]
+                          ? __ldcg(I.sic_val + static_cast<std::size_t>(step & 1) * I.N + c)
                           : I.Isic[c];
         double V = I.V[c], w = I.w[c], gex = I.gex[c], gin = I.gin[c];
         double dgex = I.dgex[c], dgin = I.dgin[c];
@@ -297,11 +297,38 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
                 I.stp_u[c] = u;
                 I.stp_t[c] = t_now;
             }
-            s_val[threadIdx.x * 2 + 0] =
+            const double v0 =
                 exc ? (I.stp_on ? I.w_e * x * u : I.w_e) : (I.stp_on ? I.w_i * x * u : I.w_i);
-            s_val[threadIdx.x * 2 + 1] = exc ? (I.stp_on ? I.w_n2a * x * u : I.w_n2a) : 0.0;
-            const int pos = atomicAdd(&s_nspk, 1);
-            s_spk[pos] = threadIdx.x;
+            const double v1 = exc ? (I.stp_on ? I.w_n2a * x * u : I.w_n2a) : 0.0;
+            if (I.deferred_push) {
+                const int ls = static_cast<int>(step % 3);
+                std::uint32_t r0, len0, len1;
+                if (exc) {
+                    r0 = I.exc_rs[c];
+                    len0 = I.exc_rs[c + 1] - r0;
+                    len1 = I.n2a_rs[c + 1] - I.n2a_rs[c];
+                } else {
+                    r0 = I.inh_rs[c - I.NE];
+                    len0 = I.inh_rs[c - I.NE + 1] - r0;
+                    len1 = 0;
+                }
+                const unsigned long long old = atomicAdd(
+                    I.spk_packed + ls, (1ull << 40) | static_cast<unsigned long long>(len0 + len1));
+                const std::size_t o = static_cast<std::size_t>(ls) * I.N + (old >> 40);
+                I.spk_meta[4 * o + 0] = c;
+                I.spk_meta[4 * o + 1] = static_cast<std::uint32_t>(old & 0xFFFFFFFFFFull);
+                I.spk_meta[4 * o + 2] = r0;
+                I.spk_meta[4 * o + 3] = len0;
+                I.spk_val[2 * o] = v0;
+                I.spk_val[2 * o + 1] = v1;
+            } else {
+                s_val[threadIdx.x * 2 + 0] = v0;
+                s_val[threadIdx.x * 2 + 1] = v1;
+            }
+            if (!I.deferred_push) {
+                const int pos = atomicAdd(&s_nspk, 1);
+                s_spk[pos] = threadIdx.x;
+            }
             if (I.rec_spikes && step >= I.rec_from) {
                 const unsigned long long li = atomicAdd(I.spike_log_n, 1ULL);
                 if (li < I.spike_log_cap) {
@@ -344,12 +371,93 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
     }
 }
 
+// Deferred push of the spikes of step-1.  The instance's PUSH blocks stride
+// over the flat edge space of that step (edge x belongs to the spike whose
+// range holds it, found by binary search in shared memory), so the work is
+// split evenly whatever the number of spikes.  One thread also clears the
+// list slot the next step appends to.
+constexpr int kPushBatch = 256;
+
+__device__ void push_role(const InstDev& I, const Work& wk, std::int64_t step) {
+    __shared__ std::uint32_t s_off[kPushBatch + 1], s_src[kPushBatch], s_r0[kPushBatch],
+        s_len0[kPushBatch];
+    __shared__ double s_v[2 * kPushBatch];
+    if (wk.first == 0 && threadIdx.x == 0) I.spk_packed[(step + 1) % 3] = 0;
+    if (step == 0) return;
+    const int ls = static_cast<int>((step - 1) % 3);
+    const unsigned long long packed = __ldcg(I.spk_packed + ls);
+    const std::uint32_t n = static_cast<std::uint32_t>(packed >> 40);
+    const std::uint32_t total = static_cast<std::uint32_t>(packed & 0xFFFFFFFFFFull);
+    const std::uint32_t stride = blockDim.x * I.push_blocks;
+    const std::uint32_t gtid = wk.first * blockDim.x + threadIdx.x;
+    const int as_e = static_cast<int>((step - 1 + I.d_e) % I.slots);
+    const int as_i = static_cast<int>((step - 1 + I.d_i) % I.slots);
+    const std::size_t base = static_cast<std::size_t>(ls) * I.N;
+    for (std::uint32_t b0 = 0; b0 < n; b0 += kPushBatch) {
+        const std::uint32_t nb = min(static_cast<std::uint32_t>(kPushBatch), n - b0);
+        __syncthreads();
+        for (std::uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+            const std::size_t o = base + b0 + i;
+            s_src[i] = __ldcg(I.spk_meta + 4 * o + 0);
+            s_off[i] = __ldcg(I.spk_meta + 4 * o + 1);
+            s_r0[i] = __ldcg(I.spk_meta + 4 * o + 2);
+            s_len0[i] = __ldcg(I.spk_meta + 4 * o + 3);
+            s_v[2 * i] = __ldcg(I.spk_val + 2 * o);
+            s_v[2 * i + 1] = __ldcg(I.spk_val + 2 * o + 1);
+        }
+        if (threadIdx.x == 0)
+            s_off[nb] = b0 + nb < n ? __ldcg(I.spk_meta + 4 * (base + b0 + nb) + 1) : total;
+        __syncthreads();
+        // The list order is the atomic order, so offsets ascend along it.
+        const std::uint32_t x0 = s_off[0], x1 = s_off[nb];
+        for (std::uint32_t x = x0 + gtid; x < x1; x += stride) {
+            std::uint32_t lo = 0, hi = nb;  // last entry with s_off <= x
+            while (hi - lo > 1) {
+                const std::uint32_t mid = (lo + hi) >> 1;
+                if (s_off[mid] <= x) lo = mid; else hi = mid;
+            }
+            const std::uint32_t j = s_src[lo];
+            std::uint32_t k = x - s_off[lo];
+            const InRing* R;
+            std::uint32_t e, t;
+            double v;
+            int slot;
+            if (j >= I.NE) {
+                R = &I.ring_in;
+                e = s_r0[lo] + k;
+                t = I.inh_tg[e];
+                v = s_v[2 * lo];
+                slot = as_i;
+            } else if (k < s_len0[lo]) {
+                R = &I.ring_ex;
+                e = s_r0[lo] + k;
+                t = I.exc_tg[e];
+                v = s_v[2 * lo];
+                slot = as_e;
+            } else {
+                R = &I.ring_as;
+                k -= s_len0[lo];
+                e = I.n2a_rs[j] + k;
+                t = I.n2a_tg[e];
+                v = s_v[2 * lo + 1];
+                slot = as_e;
+            }
+            const std::uint32_t bp = R->bitpos[e];
+            R->vals[static_cast<std::size_t>(slot) * R->words * 32 + bp] = v;
+            atomicOr(R->bits + static_cast<std::size_t>(slot) * R->words + (bp >> 5),
+                     1u << (bp & 31));
+            atomicOr(R->sum + static_cast<std::size_t>(slot) * R->n_targets + t,
+                     1ull << R->sbit[e]);
+        }
+    }
+}
+
 __device__ void astro_role(const InstDev& I, const Work& wk, std::int64_t step) {
     if (threadIdx.x >= wk.count) return;
     const std::uint32_t a = wk.first + threadIdx.x;
     const int slot = static_cast<int>(step % I.slots);
     unsigned long long* sp = I.ring_as.sum + static_cast<std::size_t>(slot) * I.ring_as.n_targets + a;
-    const unsigned long long g = *sp;
+    const unsigned long long g = __ldcg(sp);
     double ca = I.Ca[a], ip3 = I.IP3[a], hh = I.h[a];
     double ip3_in = 0.0;
     if (g != 0) {
@@ -437,12 +545,145 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restri
         neuron_role(I, wk, step);
     } else if (wk.role == kRoleAstro) {
         astro_role(I, wk, step);
+    } else if (wk.role == kRolePush) {
+        push_role(I, wk, step);
     } else {
         sic_role(I, wk, step);
     }
 }
 
+// Grid-wide barrier of the persistent chunk kernel (all blocks co-resident
+// by cooperative launch).  Sense by generation count; every wait is bounded:
+// a block that polls kBarrierPolls times without release sets the error word
+// and the whole grid stops at its next barrier, so a fault can only end the
+// launch early, never hang it.
+constexpr unsigned kBarrierPolls = 1u << 24;  // x ~64 ns sleep: ~1 s
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ bool grid_sync(GridBarrier* gb, unsigned nblocks) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = ld_acquire(&gb->gen);
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(&gb->count, 1u) == nblocks - 1) {
+            atomicExch(&gb->count, 0u);
+            __threadfence();
+            atomicAdd(&gb->gen, 1u);
+        } else {
+            unsigned polls = 0;
+            while (ld_acquire(&gb->gen) == gen) {
+                if (++polls > kBarrierPolls || ld_acquire(&gb->error) != 0) {
+                    atomicExch(&gb->error, 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (ld_acquire(&gb->error) != 0) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// All `steps` steps of a chunk in one cooperative launch: each block takes
+// work items blockIdx.x, blockIdx.x + gridDim.x, ... of every step, with a
+// grid barrier between steps.  Data other blocks wrote in earlier steps is
+// read through L2 (__ldcg in the roles), never a stale L1 line.
+__global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restrict__ insts,
+                                                          const Work* __restrict__ work,
+                                                          int n_work, int steps,
+                                                          GridBarrier* gb) {
+    __shared__ __align__(16) unsigned char s_raw[sizeof(InstDev)];
+    __shared__ unsigned s_inst;
+    if (threadIdx.x == 0) s_inst = 0xFFFFFFFFu;
+    const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
+    for (int k = 0; k < steps; ++k) {
+        for (int wi = blockIdx.x; wi < n_work; wi += gridDim.x) {
+            const Work wk = work[wi];
+            __syncthreads();
+            if (s_inst != wk.inst) {
+                const auto* src = reinterpret_cast<const std::uint32_t*>(insts + wk.inst);
+                auto* dst = reinterpret_cast<std::uint32_t*>(s_raw);
+                for (unsigned i = threadIdx.x; i < sizeof(InstDev) / 4; i += blockDim.x)
+                    dst[i] = src[i];
+                __syncthreads();
+                if (threadIdx.x == 0) s_inst = wk.inst;
+                __syncthreads();
+            }
+            const std::int64_t step = I.step0 + k;
+            if (step < I.end_step) {
+                if (wk.role == kRoleNeuron) {
+                    neuron_role(I, wk, step);
+                } else if (wk.role == kRoleAstro) {
+                    astro_role(I, wk, step);
+                } else if (wk.role == kRolePush) {
+                    push_role(I, wk, step);
+                } else {
+                    sic_role(I, wk, step);
+                }
+            }
+        }
+        if (k + 1 < steps && !grid_sync(gb, gridDim.x)) return;
+    }
+}
+
+// Failure-detection check of the bounded barrier: block 0 never arrives, so
+// every other block's wait must run out, set the error word and return.
+__global__ void barrier_selftest_kernel(GridBarrier* gb) {
+    if (blockIdx.x == 0) return;
+    grid_sync(gb, gridDim.x);
+}
+
 }  // namespace
+
+cudaError_t barrier_selftest(GridBarrier* gb, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(4);
+    cfg.blockDim = dim3(32);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, barrier_selftest_kernel, gb);
+}
+
+int persistent_blocks(int block) {
+    int per_sm = 0, dev = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chunk_kernel, block, 0) !=
+        cudaSuccess)
+        return 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return per_sm * sms;
+}
+
+cudaError_t launch_chunk_persistent(const InstDev* insts, const Work* work, int n_work,
+                                    int block, int grid, int steps, GridBarrier* gb,
+                                    cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(static_cast<unsigned>(block));
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, chunk_kernel, insts, work, n_work, steps, gb);
+}
 
 cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
                         bool pdl, cudaStream_t stream) {

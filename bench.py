@@ -154,7 +154,8 @@ def max_over_ranks(pg, x: float) -> float:
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -447,6 +448,9 @@ def main():
                     help="skip the reference CUDA kernel and sub-benchmarks")
     ap.add_argument("--skip", default="", help="comma list of sub-benchmarks to skip: "
                     "network_c2,batched_c3,serving_c4")
+    ap.add_argument("--engine-mode", type=int, default=1,
+                    help="network engine launches: 1 graphs of per-step kernels, "
+                         "2 persistent chunk kernel, -1 plain launches")
     ap.add_argument("--only", default="", choices=["", "astro", "network_c2", "batched_c3",
                                                    "serving_c4"],
                     help="run one part alone and print its JSON (profiling)")
@@ -464,7 +468,8 @@ def main():
     import torch
     torch.cuda.set_device(local)
     if args.only and args.only != "astro":
-        fn = {"network_c2": lambda: bench_network(warm=args.warmup, steps=args.steps),
+        fn = {"network_c2": lambda: bench_network(warm=args.warmup, steps=args.steps,
+                                                  use_graphs=args.engine_mode),
               "batched_c3": bench_batched, "serving_c4": bench_serving}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
         return 0

@@ -150,9 +150,14 @@ typedef struct asg_engine_opts {
     int32_t device;         /* CUDA device ordinal (default 0)                    */
     int32_t chunk_steps;    /* steps per captured CUDA graph (default 32)          */
     int32_t block;          /* threads per block of the step kernel (default 128)  */
-    int32_t use_graphs;     /* 0/1 = CUDA graphs (default), -1 = plain launches    */
+    int32_t use_graphs;     /* 0/1 = a CUDA graph of per-step launches (default),
+                               -1 = plain launches, 2 = persistent: one cooperative
+                               launch per chunk, bounded grid barrier per step    */
     int32_t sic_mode;       /* 0 auto, 1 fused into the neuron role, 2 own role    */
     int32_t pdl;            /* 0 = programmatic dependent launch (default), -1 off */
+    int32_t push_mode;      /* 0 = spikes pushed one step later by load-balanced
+                               push blocks when both spike delays are >= 2 steps
+                               (default), 1 = pushed by the spiking block      */
     uint64_t mem_budget;    /* device bytes the engine may hold (0 = 90% free)     */
 } asg_engine_opts;
 
@@ -308,6 +313,12 @@ int asg_astro_update_noalloc(uint32_t n, double* Ca, double* IP3, double* h, dou
                              int32_t substeps, double noise_std, int32_t independent_noise,
                              double shared_noise, uint64_t noise_seed, uint64_t noise_index,
                              void* stream);
+
+/* Failure-detection self-test of the bounded device waits: launches a grid in
+ * which one block never reaches the grid barrier; the others must give up
+ * within about a second, set the error word and return.  *timed_out = 1 when
+ * they did; *wait_ms is the launch's device time.  The context stays usable. */
+int asg_selftest_barrier_timeout(int32_t* timed_out, double* wait_ms);
 
 /* ------------------------------------------ host side: config + builder
  * The reference's JSON schema (parameters.cpp:85-205): '//' comments, key

@@ -1,0 +1,60 @@
+"""Failure detection without faulting the GPU: bounded device waits return an
+error status the host reads (the context stays usable), and host-side
+failures (allocation refused, bad input) come back as status codes."""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from astrosimgpu_b200 import _lib
+from astrosimgpu_b200.network import Model, Network, config_path
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_grid_barrier_wait_is_bounded_and_reported():
+    lib = _lib.load()
+    t = C.c_int32()
+    ms = C.c_double()
+    assert lib.asg_selftest_barrier_timeout(C.byref(t), C.byref(ms)) == 0
+    assert t.value == 1            # the blocks gave up and said so
+    assert ms.value < 20000.0      # within the bound, no hang
+    # the context is still usable afterwards
+    n = Network(Model(config_path("quick"), pre_time=0.0), use_graphs=2)
+    n.step(100)
+    assert np.isfinite(n.state()["V"]).all()
+
+
+def test_injected_allocation_failure_is_a_status():
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "from astrosimgpu_b200 import _lib\n"
+        "from astrosimgpu_b200.network import Model, Network, config_path\n"
+        "m = Model(config_path('use_case'))\n"
+        "try:\n"
+        "    Network(m)\n"
+        "    print('created')\n"
+        "except _lib.AsgError as e:\n"
+        "    print('status', e.status)\n" % ROOT)
+    env = dict(os.environ, ASG_FAIL_ALLOC_AFTER="1")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert "status 2" in out.stdout  # ASG_ERR_OOM, no abort
+
+
+def test_unsupported_per_edge_weights_rejected():
+    m = Model(config_path("quick"), pre_time=0.0)
+    d = m.desc()
+    rs, tg = m.table(0)
+    w = np.full(len(tg), 5.0)
+    w[3] = 4.0
+    bad = _lib.NetworkDesc.from_buffer_copy(d)
+    bad.exc_primary.weight = _lib.dptr(w)
+    h = C.c_void_p()
+    st = _lib.load().asg_create(C.byref(bad), None, None, C.byref(h))
+    assert st == 4 and b"weight" in _lib.load().asg_last_error()

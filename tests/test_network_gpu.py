@@ -120,6 +120,10 @@ def variants():
     v["astrocyte"]["IP3"] = 0.6
     v["connectivity"].update({"pool_type": "random", "pool_size": 5, "p_third_if_primary": 0.6})
     out.append(("active_astrocytes_random_pools", v))
+    v = json.loads(json.dumps(base))
+    v["synapse"]["d_e"] = 0.1  # one-step spike delay: pushes stay in the spiking block
+    v["synapse"]["d_i"] = 0.2
+    out.append(("one_step_spike_delay", v))
     return out
 
 
@@ -133,13 +137,17 @@ def test_variant_parity(label, cfg):
 
 
 def test_sic_modes_and_block_sizes_bitwise():
-    """The separate SIC role and the fused form, and any block size, give
+    """The separate SIC role and the fused form, any block size, per-step
+    graph launches, plain launches and the persistent chunk kernel give
     identical bits (the arithmetic per cell does not depend on the launch)."""
     path = config_path("use_case")
     m = Model(path, pre_time=0.0)
     outs = []
     for opts in (dict(sic_mode=1, block=64), dict(sic_mode=2, block=256),
-                 dict(sic_mode=0, block=128, chunk_steps=7, use_graphs=-1)):
+                 dict(sic_mode=0, block=128, chunk_steps=7, use_graphs=-1),
+                 dict(block=128, chunk_steps=50, use_graphs=2),
+                 dict(block=64, chunk_steps=13, use_graphs=2, pdl=-1),
+                 dict(block=96, chunk_steps=32, push_mode=1)):
         n = Network(m, record=rec_all(), **opts)
         n.step(1200)
         outs.append((n.fetch_spikes(), n.state()))
@@ -149,13 +157,14 @@ def test_sic_modes_and_block_sizes_bitwise():
             assert np.array_equal(st[k], outs[0][1][k]), k
 
 
-def test_batch_equals_single_bitwise():
+@pytest.mark.parametrize("mode", [1, 2])
+def test_batch_equals_single_bitwise(mode):
     """Instances of uneven size packed into one engine give the bits each
-    gives alone."""
+    gives alone (graph launches and the persistent chunk kernel)."""
     names = ["quick", "use_case", "quick", "bursting"]
     seeds = [1, 2, 3, 4]
     models = [Model(config_path(n), seed=s, pre_time=0.0) for n, s in zip(names, seeds)]
-    b = Batch(models, record=rec_all())
+    b = Batch(models, record=rec_all(), use_graphs=mode)
     b.step(800)
     for i, m in enumerate(models):
         n = Network(m, record=rec_all())
