@@ -144,6 +144,7 @@ SIGNATURES = {
     "asg_checkpoint": (C.c_int, [vp, vp, C.c_uint64]),
     "asg_restore": (C.c_int, [vp, vp, C.c_uint64]),
     "asg_destroy": (C.c_int, [vp]),
+    "asg_autotune": (C.c_int, [vp, C.c_int32, C.POINTER(EngineOpts)]),
     # batch
     "asg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(NetworkDesc)),
                                    C.POINTER(RecordOpts), C.POINTER(EngineOpts), vpp]),

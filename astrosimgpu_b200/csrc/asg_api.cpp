@@ -89,6 +89,105 @@ struct BatchHandle {
     std::vector<int> ids;
 };
 
+// Times candidate launch shapes on a snapshot of every instance (device
+// arena + host bookkeeping restored after each trial, so the simulation is
+// not advanced) and keeps the fastest: chunk length x block size x launch
+// mode (CUDA graph of per-step launches or the persistent chunk kernel).
+int autotune_engine(Engine& e, int32_t steps, asg_engine_opts* chosen) {
+    ASG_TRY(e.flush());
+    // Snapshot every instance (device arena + host-side bookkeeping).
+    struct Snap {
+        DevBuf copy;
+        int64_t step;
+        std::size_t spikes, arows, nrows, ca, ip3, v, isic;
+        int64_t se, sic, ns;
+    };
+    std::vector<Snap> snaps(e.insts.size());
+    for (std::size_t i = 0; i < e.insts.size(); ++i) {
+        Instance& I = *e.insts[i];
+        Snap& s = snaps[i];
+        ASG_TRY(s.copy.alloc(I.arena_bytes, false));
+        ASG_CUDA(cudaMemcpyAsync(s.copy.get(), I.arena.get(), I.arena_bytes,
+                                 cudaMemcpyDeviceToDevice, e.stream));
+        s.step = I.step;
+        s.spikes = I.spikes.size();
+        s.arows = I.astro_rec_steps.size();
+        s.nrows = I.neuron_rec_steps.size();
+        s.ca = I.rec_Ca.size();
+        s.ip3 = I.rec_IP3.size();
+        s.v = I.rec_V.size();
+        s.isic = I.rec_Isic.size();
+        s.se = I.spike_edges;
+        s.sic = I.sic_edges;
+        s.ns = I.n_spikes;
+    }
+    ASG_CUDA(cudaStreamSynchronize(e.stream));
+    auto restore = [&]() -> int {
+        ASG_TRY(e.flush());
+        for (std::size_t i = 0; i < e.insts.size(); ++i) {
+            Instance& I = *e.insts[i];
+            Snap& s = snaps[i];
+            ASG_CUDA(cudaMemcpyAsync(I.arena.get(), s.copy.get(), I.arena_bytes,
+                                     cudaMemcpyDeviceToDevice, e.stream));
+            I.step = s.step;
+            I.spikes.resize(s.spikes);
+            I.astro_rec_steps.resize(s.arows);
+            I.neuron_rec_steps.resize(s.nrows);
+            I.rec_Ca.resize(s.ca);
+            I.rec_IP3.resize(s.ip3);
+            I.rec_V.resize(s.v);
+            I.rec_Isic.resize(s.isic);
+            I.spike_edges = s.se;
+            I.sic_edges = s.sic;
+            I.n_spikes = s.ns;
+        }
+        ASG_CUDA(cudaStreamSynchronize(e.stream));
+        return ASG_OK;
+    };
+    const int block0 = e.cfg.block, chunk0 = e.cfg.chunk_steps, mode0 = e.cfg.use_graphs;
+    int best_block = block0, best_chunk = chunk0, best_mode = mode0;
+    double best = 1e300;
+    for (int mode : {1, 2}) {
+        for (int chunk : {32, 64, 128}) {
+            if (e.set_chunk(chunk) != ASG_OK) continue;
+            for (int block : {128, 256, 512}) {
+                ASG_TRY(e.set_block(block));
+                ASG_TRY(e.set_mode(mode));
+                ASG_TRY(e.run(std::max(steps / 4, 1)));  // warm: graph build, caches
+                ASG_TRY(restore());
+                ASG_TRY(e.run(steps));
+                const double per = e.last_ms / steps;
+                if (per < best) {
+                    best = per;
+                    best_block = block;
+                    best_chunk = chunk;
+                    best_mode = mode;
+                }
+                ASG_TRY(restore());
+            }
+        }
+    }
+    clear_error();
+    ASG_TRY(e.set_chunk(best_chunk));
+    ASG_TRY(e.set_block(best_block));
+    ASG_TRY(e.set_mode(best_mode));
+    if (chosen != nullptr) {
+        std::memset(chosen, 0, sizeof *chosen);
+        chosen->device = e.cfg.device;
+        chosen->chunk_steps = best_chunk;
+        chosen->block = best_block;
+        chosen->use_graphs = best_mode;
+        chosen->sic_mode = e.cfg.sic_mode;
+        chosen->pdl = e.cfg.pdl ? 0 : -1;
+        chosen->push_mode = e.cfg.push_mode;
+        chosen->mem_budget = e.cfg.mem_budget;
+    }
+    (void)block0;
+    (void)mode0;
+    return ASG_OK;
+}
+
+
 }  // namespace asg
 
 using asg::BatchHandle;
@@ -309,92 +408,13 @@ int asg_batch_last_timing(asg_batch* b, double* device_ms, int64_t* kernels) {
 int asg_batch_autotune(asg_batch* b, int32_t steps, asg_engine_opts* chosen) {
     asg::clear_error();
     if (b == nullptr || steps <= 0) return asg::fail(ASG_ERR_ARG, "asg_batch_autotune: bad arguments");
-    Engine& e = *reinterpret_cast<BatchHandle*>(b)->eng;
-    ASG_TRY(e.flush());
-    // Snapshot every instance (device arena + host-side bookkeeping).
-    struct Snap {
-        asg::DevBuf copy;
-        int64_t step;
-        std::size_t spikes, arows, nrows, ca, ip3, v, isic;
-        int64_t se, sic, ns;
-    };
-    std::vector<Snap> snaps(e.insts.size());
-    for (std::size_t i = 0; i < e.insts.size(); ++i) {
-        asg::Instance& I = *e.insts[i];
-        Snap& s = snaps[i];
-        ASG_TRY(s.copy.alloc(I.arena_bytes, false));
-        ASG_CUDA(cudaMemcpyAsync(s.copy.get(), I.arena.get(), I.arena_bytes,
-                                 cudaMemcpyDeviceToDevice, e.stream));
-        s.step = I.step;
-        s.spikes = I.spikes.size();
-        s.arows = I.astro_rec_steps.size();
-        s.nrows = I.neuron_rec_steps.size();
-        s.ca = I.rec_Ca.size();
-        s.ip3 = I.rec_IP3.size();
-        s.v = I.rec_V.size();
-        s.isic = I.rec_Isic.size();
-        s.se = I.spike_edges;
-        s.sic = I.sic_edges;
-        s.ns = I.n_spikes;
-    }
-    ASG_CUDA(cudaStreamSynchronize(e.stream));
-    auto restore = [&]() -> int {
-        ASG_TRY(e.flush());
-        for (std::size_t i = 0; i < e.insts.size(); ++i) {
-            asg::Instance& I = *e.insts[i];
-            Snap& s = snaps[i];
-            ASG_CUDA(cudaMemcpyAsync(I.arena.get(), s.copy.get(), I.arena_bytes,
-                                     cudaMemcpyDeviceToDevice, e.stream));
-            I.step = s.step;
-            I.spikes.resize(s.spikes);
-            I.astro_rec_steps.resize(s.arows);
-            I.neuron_rec_steps.resize(s.nrows);
-            I.rec_Ca.resize(s.ca);
-            I.rec_IP3.resize(s.ip3);
-            I.rec_V.resize(s.v);
-            I.rec_Isic.resize(s.isic);
-            I.spike_edges = s.se;
-            I.sic_edges = s.sic;
-            I.n_spikes = s.ns;
-        }
-        ASG_CUDA(cudaStreamSynchronize(e.stream));
-        return ASG_OK;
-    };
-    const int block0 = e.cfg.block, chunk0 = e.cfg.chunk_steps;
-    int best_block = block0, best_chunk = chunk0;
-    double best = 1e300;
-    for (int chunk : {16, 32, 64, 128}) {
-        if (e.set_chunk(chunk) != ASG_OK) continue;
-        for (int block : {64, 128, 256, 512}) {
-            ASG_TRY(e.set_block(block));
-            ASG_TRY(e.run(std::max(steps / 4, 1)));  // warm: graph build, caches
-            ASG_TRY(restore());
-            ASG_TRY(e.run(steps));
-            const double per = e.last_ms / steps;
-            if (per < best) {
-                best = per;
-                best_block = block;
-                best_chunk = chunk;
-            }
-            ASG_TRY(restore());
-        }
-    }
+    return asg::autotune_engine(*reinterpret_cast<BatchHandle*>(b)->eng, steps, chosen);
+}
+
+int asg_autotune(asg_network* net, int32_t steps, asg_engine_opts* chosen) {
     asg::clear_error();
-    ASG_TRY(e.set_chunk(best_chunk));
-    ASG_TRY(e.set_block(best_block));
-    if (chosen != nullptr) {
-        std::memset(chosen, 0, sizeof *chosen);
-        chosen->device = e.cfg.device;
-        chosen->chunk_steps = best_chunk;
-        chosen->block = best_block;
-        chosen->use_graphs = e.cfg.use_graphs;
-        chosen->sic_mode = e.cfg.sic_mode;
-        chosen->pdl = e.cfg.pdl ? 0 : -1;
-        chosen->push_mode = e.cfg.push_mode;
-        chosen->mem_budget = e.cfg.mem_budget;
-    }
-    (void)block0;
-    return ASG_OK;
+    if (net == nullptr || steps <= 0) return asg::fail(ASG_ERR_ARG, "asg_autotune: bad arguments");
+    return asg::autotune_engine(*reinterpret_cast<NetworkHandle*>(net)->eng, steps, chosen);
 }
 
 int asg_batch_destroy(asg_batch* b) {

@@ -76,8 +76,8 @@ AstroK make_astro_k(const asg_astro_params& a, double h, int substeps) {
 // in-edges are numbered p = 0.. in (source, row position) order; bit p of the
 // target's words marks an arrival on that edge.
 struct InRingHost {
-    std::vector<std::uint32_t> wbase, bitpos;
-    std::vector<std::uint8_t> sbit;
+    std::vector<std::uint32_t> wbase;
+    std::vector<unsigned long long> edge;  // bit | target << 32 | summary bit << 58
     std::uint32_t words = 0;
 };
 
@@ -90,8 +90,7 @@ InRingHost make_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std:
     r.wbase.assign(n_targets + 1, 0);
     for (std::uint32_t t = 0; t < n_targets; ++t) r.wbase[t + 1] = r.wbase[t] + (deg[t] + 31) / 32;
     r.words = r.wbase[n_targets];
-    r.bitpos.assign(m, 0);
-    r.sbit.assign(m, 0);
+    r.edge.assign(m, 0);
     std::vector<std::uint32_t> next(n_targets, 0);
     // Sources ascending, each row in CSR order: in-edge numbers follow
     // (source, position in the source's row).
@@ -101,8 +100,9 @@ InRingHost make_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std:
             const std::uint32_t p = next[t]++;
             const std::uint32_t nw = r.wbase[t + 1] - r.wbase[t];
             const std::uint32_t G = (nw + 63) / 64;
-            r.bitpos[e] = r.wbase[t] * 32 + p;
-            r.sbit[e] = static_cast<std::uint8_t>((p / 32) / G);
+            const unsigned long long bit = static_cast<unsigned long long>(r.wbase[t]) * 32 + p;
+            r.edge[e] = bit | (static_cast<unsigned long long>(t) << 32) |
+                        (static_cast<unsigned long long>((p / 32) / G) << 58);
         }
     }
     return r;
@@ -305,6 +305,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     if (!delay_ok(d.d_e_steps) || !delay_ok(d.d_i_steps) || !delay_ok(d.d_a2n_steps))
         return fail(ASG_ERR_ARG, "delays must be at least one step");
     if (NA >= (1u << 24)) return fail(ASG_ERR_UNSUPPORTED, "at most 2^24-1 astrocytes");
+    if (NE + NI >= (1u << 26)) return fail(ASG_ERR_UNSUPPORTED, "at most 2^26-1 neurons");
     if (N > 0 && (d.V_reset == nullptr || d.b == nullptr))
         return fail(ASG_ERR_ARG, "per-cell V_reset and b are required");
     if (first < 0 || end < first) return fail(ASG_ERR_ARG, "bad step range");
@@ -339,8 +340,10 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     // Deferred push needs both spike delays >= 2 steps (the push of step s
     // runs in step s+1 and must land before step s+d reads it).
     D.deferred_push = (cfg.push_mode != 1 && d.d_e_steps >= 2 && d.d_i_steps >= 2) ? 1 : 0;
-    D.push_blocks = static_cast<std::int32_t>(
-        std::min<std::uint32_t>(128, std::max<std::uint32_t>(1, (N + 255) / 256)));
+    // Enough push threads for a synchronous burst (every edge of a large
+    // fraction of the network in one step), at most two blocks per SM.
+    D.push_blocks = static_cast<std::int32_t>(std::min<std::uint32_t>(
+        2u * static_cast<std::uint32_t>(sms), std::max<std::uint32_t>(1, (N + 63) / 64)));
     D.seed = d.seed;
     D.dt = d.dt;
     const double h = d.dt / static_cast<double>(d.substeps);
@@ -425,9 +428,6 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
 
     const std::size_t S = static_cast<std::size_t>(D.slots);
     const std::size_t n8 = static_cast<std::size_t>(N) * 8, a8 = static_cast<std::size_t>(NA) * 8;
-    auto e4 = [](const asg_csr& c) {
-        return static_cast<std::size_t>(c.n_sources ? c.row_start[c.n_sources] : 0) * 4;
-    };
     std::vector<Seg> segs;
     auto add_seg = [&](auto*& dst, std::size_t bytes, const void* src) {
         segs.push_back(Seg{static_cast<void*>(&dst), bytes, src});
@@ -459,16 +459,12 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     add_seg(D.stp_u, n8, stp_u.data());
     add_seg(D.stp_t, n8, stp_t.data());
     add_seg(D.exc_rs, (NE + 1) * 4, d.exc_primary.n_sources ? d.exc_primary.row_start : zero_rs);
-    add_seg(D.exc_tg, e4(d.exc_primary), d.exc_primary.target);
     add_seg(D.inh_rs, (NI + 1) * 4, d.inh_primary.n_sources ? d.inh_primary.row_start : zero_rs);
-    add_seg(D.inh_tg, e4(d.inh_primary), d.inh_primary.target);
     add_seg(D.n2a_rs, (NE + 1) * 4, d.neuron_astro.n_sources ? d.neuron_astro.row_start : zero_rs);
-    add_seg(D.n2a_tg, e4(d.neuron_astro), d.neuron_astro.target);
     auto ring_segs = [&](InRing& R, InRingHost& H, std::uint32_t n_t) {
         const std::size_t W = std::max<std::uint32_t>(H.words, 1);
         add_seg(R.wbase, H.wbase.size() * 4, H.wbase.data());
-        add_seg(R.bitpos, H.bitpos.size() * 4, H.bitpos.data());
-        add_seg(R.sbit, H.sbit.size(), H.sbit.data());
+        add_seg(R.edge, H.edge.size() * 8, H.edge.data());
         add_seg(R.bits, S * W * 4, nullptr);
         add_seg(R.sum, S * std::max<std::uint32_t>(n_t, 1) * 8, nullptr);
         add_seg(R.vals, S * W * 32 * 8, nullptr);
@@ -571,6 +567,14 @@ int Engine::set_block(int block) {
     if (block < 32 || block > 512 || block % 32)
         return fail(ASG_ERR_ARG, "block size %d must be a multiple of 32 in [32, 512]", block);
     cfg.block = block;
+    dirty = true;
+    return ASG_OK;
+}
+
+int Engine::set_mode(int use_graphs) {
+    if (use_graphs != -1 && use_graphs != 0 && use_graphs != 1 && use_graphs != 2)
+        return fail(ASG_ERR_ARG, "launch mode %d is not -1, 0, 1 or 2", use_graphs);
+    cfg.use_graphs = use_graphs;
     dirty = true;
     return ASG_OK;
 }

@@ -60,8 +60,9 @@ struct Work {
 // Incoming-edge structure of one arrival ring (transpose of a source CSR).
 struct InRing {
     const std::uint32_t* wbase;   // [n_targets+1] first bitmap word of each target
-    const std::uint32_t* bitpos;  // [E] bit index of each OUT-edge (source CSR order)
-    const std::uint8_t* sbit;     // [E] summary bit of that edge's word group
+    // [E] per OUT-edge (source CSR order): bit index | target << 32 | summary
+    // bit << 58 -- one 8-byte load gives everything a push needs.
+    const unsigned long long* edge;
     std::uint32_t* bits;          // [slots][words] arrival bitmaps
     unsigned long long* sum;      // [slots][n_targets] non-empty word groups
     double* vals;                 // [slots][words*32] value at each set bit
@@ -101,8 +102,9 @@ struct InstDev {
     double inv_tau_rec, inv_tau_fac;  // correctly rounded reciprocals (div_by)
     // STP per source
     double *stp_x, *stp_u, *stp_t;
-    // out-edge CSR (source order) of the three spike-carrying sets
-    const std::uint32_t *exc_rs, *exc_tg, *inh_rs, *inh_tg, *n2a_rs, *n2a_tg;
+    // row starts of the three spike-carrying sets (source CSR order); the
+    // edges themselves are the rings' packed `edge` words
+    const std::uint32_t *exc_rs, *inh_rs, *n2a_rs;
     InRing ring_ex, ring_in, ring_as;
     // Deferred push (both spike delays >= 2 steps): each spike of step s
     // reserves a contiguous range of that step's flat edge space (one 64-bit

@@ -103,6 +103,7 @@ public:
 
     int set_block(int block);
     int set_chunk(int chunk);
+    int set_mode(int use_graphs);
 
 private:
     int rebuild();          // work table + graph after the instance set changed

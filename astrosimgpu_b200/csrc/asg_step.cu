@@ -128,23 +128,25 @@ __device__ __forceinline__ double sic_sum(const InstDev& I, std::uint32_t t, int
     return acc;
 }
 
-// Writes `value` at the bit of each out-edge of `row` in `slot`, sets the
-// bit and the target's summary bit.
-__device__ __forceinline__ void push_row(const std::uint32_t* rs, const std::uint32_t* tg,
-                                         const InRing& R, std::uint32_t row, int slot,
-                                         double value) {
-    std::uint32_t* bits = R.bits + static_cast<std::size_t>(slot) * R.words;
-    unsigned long long* sum = R.sum + static_cast<std::size_t>(slot) * R.n_targets;
-    double* vals = R.vals + static_cast<std::size_t>(slot) * R.words * 32;
+// One arrival: value at the edge's bit, the bit, the target's summary bit.
+__device__ __forceinline__ void push_edge(const InRing& R, int slot, unsigned long long pe,
+                                          double value) {
+    const std::uint32_t b = static_cast<std::uint32_t>(pe);
+    const std::uint32_t t = static_cast<std::uint32_t>(pe >> 32) & 0x3FFFFFFu;
+    const std::uint32_t g = static_cast<std::uint32_t>(pe >> 58);
+    R.vals[static_cast<std::size_t>(slot) * R.words * 32 + b] = value;
+    atomicOr(R.bits + static_cast<std::size_t>(slot) * R.words + (b >> 5), 1u << (b & 31));
+    atomicOr(R.sum + static_cast<std::size_t>(slot) * R.n_targets + t, 1ull << g);
+}
+
+// Writes `value` at every out-edge of `row` (in-block push, used when a
+// spike delay is a single step).
+__device__ __forceinline__ void push_row(const std::uint32_t* rs, const InRing& R,
+                                         std::uint32_t row, int slot, double value) {
     const std::uint32_t e1 = rs[row + 1];
 #pragma unroll 4
-    for (std::uint32_t e = rs[row] + threadIdx.x; e < e1; e += blockDim.x) {
-        const std::uint32_t t = tg[e];
-        const std::uint32_t b = R.bitpos[e];
-        vals[b] = value;
-        atomicOr(bits + (b >> 5), 1u << (b & 31));
-        atomicOr(sum + t, 1ull << R.sbit[e]);
-    }
+    for (std::uint32_t e = rs[row] + threadIdx.x; e < e1; e += blockDim.x)
+        push_edge(R, slot, __ldg(R.edge + e), value);
 }
 
 __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step) {
@@ -362,11 +364,11 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
         const std::uint32_t j = wk.first + lane;
         if (j < I.NE) {
             const int as = static_cast<int>((step + I.d_e) % I.slots);
-            push_row(I.exc_rs, I.exc_tg, I.ring_ex, j, as, s_val[2 * lane]);
-            push_row(I.n2a_rs, I.n2a_tg, I.ring_as, j, as, s_val[2 * lane + 1]);
+            push_row(I.exc_rs, I.ring_ex, j, as, s_val[2 * lane]);
+            push_row(I.n2a_rs, I.ring_as, j, as, s_val[2 * lane + 1]);
         } else {
             const int as = static_cast<int>((step + I.d_i) % I.slots);
-            push_row(I.inh_rs, I.inh_tg, I.ring_in, j - I.NE, as, s_val[2 * lane]);
+            push_row(I.inh_rs, I.ring_in, j - I.NE, as, s_val[2 * lane]);
         }
     }
 }
@@ -410,6 +412,7 @@ __device__ void push_role(const InstDev& I, const Work& wk, std::int64_t step) {
         __syncthreads();
         // The list order is the atomic order, so offsets ascend along it.
         const std::uint32_t x0 = s_off[0], x1 = s_off[nb];
+#pragma unroll 4
         for (std::uint32_t x = x0 + gtid; x < x1; x += stride) {
             std::uint32_t lo = 0, hi = nb;  // last entry with s_off <= x
             while (hi - lo > 1) {
@@ -417,37 +420,15 @@ __device__ void push_role(const InstDev& I, const Work& wk, std::int64_t step) {
                 if (s_off[mid] <= x) lo = mid; else hi = mid;
             }
             const std::uint32_t j = s_src[lo];
-            std::uint32_t k = x - s_off[lo];
-            const InRing* R;
-            std::uint32_t e, t;
-            double v;
-            int slot;
+            const std::uint32_t k = x - s_off[lo];
             if (j >= I.NE) {
-                R = &I.ring_in;
-                e = s_r0[lo] + k;
-                t = I.inh_tg[e];
-                v = s_v[2 * lo];
-                slot = as_i;
+                push_edge(I.ring_in, as_i, __ldg(I.ring_in.edge + s_r0[lo] + k), s_v[2 * lo]);
             } else if (k < s_len0[lo]) {
-                R = &I.ring_ex;
-                e = s_r0[lo] + k;
-                t = I.exc_tg[e];
-                v = s_v[2 * lo];
-                slot = as_e;
+                push_edge(I.ring_ex, as_e, __ldg(I.ring_ex.edge + s_r0[lo] + k), s_v[2 * lo]);
             } else {
-                R = &I.ring_as;
-                k -= s_len0[lo];
-                e = I.n2a_rs[j] + k;
-                t = I.n2a_tg[e];
-                v = s_v[2 * lo + 1];
-                slot = as_e;
+                push_edge(I.ring_as, as_e, __ldg(I.ring_as.edge + I.n2a_rs[j] + (k - s_len0[lo])),
+                          s_v[2 * lo + 1]);
             }
-            const std::uint32_t bp = R->bitpos[e];
-            R->vals[static_cast<std::size_t>(slot) * R->words * 32 + bp] = v;
-            atomicOr(R->bits + static_cast<std::size_t>(slot) * R->words + (bp >> 5),
-                     1u << (bp & 31));
-            atomicOr(R->sum + static_cast<std::size_t>(slot) * R->n_targets + t,
-                     1ull << R->sbit[e]);
         }
     }
 }

@@ -189,6 +189,12 @@ class Network:
         _lib.call("asg_last_timing", self._h, C.byref(ms), C.byref(k))
         return ms.value, k.value
 
+    def autotune(self, steps=64):
+        """Pick the fastest launch shape on a snapshot (state unchanged)."""
+        o = _lib.EngineOpts()
+        _lib.call("asg_autotune", self._h, int(steps), C.byref(o))
+        return {f: getattr(o, f) for f, _ in _lib.EngineOpts._fields_}
+
     def checkpoint(self) -> bytes:
         n = C.c_uint64()
         _lib.call("asg_checkpoint_size", self._h, C.byref(n))

@@ -258,7 +258,7 @@ def bench_astro_scaling(args, rank, world, pg):
     return out, (w, Ca, IP3, h)
 
 
-def bench_network(name="paper_sparse_dt005", warm=200, steps=2000, **opts):
+def bench_network(name="paper_sparse_dt005", warm=400, steps=2000, autotune=True, **opts):
     """Plain one-network path on a shipped config: device time per step."""
     from astrosimgpu_b200 import _lib
     from astrosimgpu_b200.network import Model, Network, config_path
@@ -267,6 +267,7 @@ def bench_network(name="paper_sparse_dt005", warm=200, steps=2000, **opts):
     build_s = time.perf_counter() - t0
     net = Network(m, record=_lib.RecordOpts(0, 10, 1, 0, 0), **opts)
     net.step(warm)
+    tuned = net.autotune(200) if autotune else None
     c0 = net.counters()
     net.step(steps)
     ms, kernels = net.last_timing()
@@ -278,7 +279,8 @@ def bench_network(name="paper_sparse_dt005", warm=200, steps=2000, **opts):
             "us_per_step": us, "neuron_updates_per_s": n / (us * 1e-6),
             "synaptic_events_per_s": events / (ms * 1e-3),
             "sim_s_per_wall_s": (m.dt * 1e-3) / (us * 1e-6), "kernels": kernels,
-            "spikes": c1["spikes"] - c0["spikes"], "build_s": build_s, "steps": steps}
+            "spikes": c1["spikes"] - c0["spikes"], "build_s": build_s, "steps": steps,
+            "warm_steps": warm, "autotuned": tuned}
 
 
 def bench_batched(sim_ms=500.0, n_inst=64, autotune=True):
@@ -448,9 +450,9 @@ def main():
                     help="skip the reference CUDA kernel and sub-benchmarks")
     ap.add_argument("--skip", default="", help="comma list of sub-benchmarks to skip: "
                     "network_c2,batched_c3,serving_c4")
-    ap.add_argument("--engine-mode", type=int, default=1,
-                    help="network engine launches: 1 graphs of per-step kernels, "
-                         "2 persistent chunk kernel, -1 plain launches")
+    ap.add_argument("--engine-mode", type=int, default=0,
+                    help="network engine launches (--only network_c2): 0 autotune, 1 graphs "
+                         "of per-step kernels, 2 persistent chunk kernel")
     ap.add_argument("--only", default="", choices=["", "astro", "network_c2", "batched_c3",
                                                    "serving_c4"],
                     help="run one part alone and print its JSON (profiling)")
@@ -469,7 +471,8 @@ def main():
     torch.cuda.set_device(local)
     if args.only and args.only != "astro":
         fn = {"network_c2": lambda: bench_network(warm=args.warmup, steps=args.steps,
-                                                  use_graphs=args.engine_mode),
+                                                  autotune=args.engine_mode == 0,
+                                                  use_graphs=max(args.engine_mode, 1)),
               "batched_c3": bench_batched, "serving_c4": bench_serving}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
         return 0

@@ -171,6 +171,11 @@ int asg_create(const asg_network_desc* desc, const asg_record_opts* rec,
 /* Advance n_steps from the handle's current step. */
 int asg_step(asg_network* net, int64_t n_steps);
 int asg_current_step(asg_network* net, int64_t* step);
+/* Time launch shapes (chunk length, block size, graph vs persistent launch)
+ * for `steps` steps on a snapshot of the network (restored after each trial:
+ * the simulation does not advance) and keep the fastest; *chosen (may be NULL)
+ * receives it.  The batched form has asg_batch_autotune. */
+int asg_autotune(asg_network* net, int32_t steps, asg_engine_opts* chosen);
 /* Spikes emitted since the last fetch, sorted by (step, source).  *count is
  * the number available; ASG_ERR_OVERFLOW (nothing consumed) if > cap. */
 int asg_fetch_spikes(asg_network* net, int64_t* steps, uint32_t* sources, int64_t cap,
