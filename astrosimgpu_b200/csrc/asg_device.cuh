@@ -73,6 +73,9 @@ __device__ __forceinline__ double normal_clamped(std::uint64_t seed, std::uint64
     return sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
 }
 
+static __device__ __noinline__ int poisson_large(std::uint64_t seed, std::uint64_t stream,
+                                                 std::uint64_t counter, double lambda);
+
 // Sequential draws of one (seed, stream), the CounterRng object form.
 struct Draws {
     std::uint64_t seed, stream, counter;
@@ -91,13 +94,12 @@ struct Draws {
         return sqrt(-2.0 * log(u1)) * cos(kTwoPi * u2);
     }
     // Knuth's product method for lambda <= 30 with exp(-lambda) supplied by
-    // the caller (a per-population constant); normal approximation above.
+    // the caller (a per-population constant); normal approximation above,
+    // out of line (rare, and it carries log/cos code the common path does
+    // not need in the instruction cache).  The object is not used after.
     __device__ __forceinline__ int poisson(double lambda, double limit) {
         if (lambda <= 0.0) return 0;
-        if (lambda > 30.0) {
-            const double v = lambda + sqrt(lambda) * normal_first();
-            return v < 0.0 ? 0 : static_cast<int>(v + 0.5);
-        }
+        if (lambda > 30.0) return poisson_large(seed, stream, counter, lambda);
         double product = uniform();
         int count = 0;
         while (product > limit) {
@@ -107,6 +109,16 @@ struct Draws {
         return count;
     }
 };
+
+// Normal approximation of Poisson(lambda) for lambda > 30 (rng.hpp:111-114):
+// round(lambda + sqrt(lambda) * N(0,1)), clamped at zero.
+static __device__ __noinline__ int poisson_large(std::uint64_t seed, std::uint64_t stream,
+                                                 std::uint64_t counter, double lambda) {
+    Draws r(seed, stream);
+    r.counter = counter;
+    const double v = lambda + sqrt(lambda) * r.normal_first();
+    return v < 0.0 ? 0 : static_cast<int>(v + 0.5);
+}
 
 // ------------------------------------------------------------- division
 

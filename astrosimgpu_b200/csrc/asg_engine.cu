@@ -108,13 +108,30 @@ InRingHost make_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std:
     return r;
 }
 
-// Compressed SIC lists in sliced ELL (32 targets per slice).
+// Compressed SIC lists in sliced ELL (32 targets per slice), each target's
+// list cut into `parts` consecutive pieces of about equal edge count (an
+// (astrocyte, multiplicity) pair that straddles a cut is split in two: m1
+// then m2 equal additions are the m additions).
 struct SicHost {
     std::vector<std::uint32_t> soff, ent;
+    std::uint32_t max_edges = 0;  // largest number of SIC edges of one target
 };
 
+constexpr std::uint32_t kSicEdgesPerPart = 256;
+constexpr std::uint32_t kPushCells = 256;
+
+// Longest SIC edge list of one target (sets the number of parts).
+std::uint32_t sic_max_edges(std::uint32_t NA, const std::uint32_t* rs, const std::uint32_t* tg,
+                            std::uint32_t N) {
+    std::vector<std::uint32_t> deg(N, 0);
+    for (std::uint32_t e = 0; e < rs[NA]; ++e) deg[tg[e]]++;
+    std::uint32_t mx = 0;
+    for (std::uint32_t d : deg) mx = std::max(mx, d);
+    return mx;
+}
+
 SicHost make_sic(std::uint32_t NA, const std::uint32_t* rs, const std::uint32_t* tg,
-                 std::uint32_t N) {
+                 std::uint32_t N, std::uint32_t parts, std::uint32_t npad) {
     // per target: (astro, mult) in ascending astro order
     std::vector<std::vector<std::uint32_t>> lists(N);
     for (std::uint32_t a = 0; a < NA; ++a) {
@@ -127,20 +144,45 @@ SicHost make_sic(std::uint32_t NA, const std::uint32_t* rs, const std::uint32_t*
             }
         }
     }
+    // Split each target's list at edge counts floor(p * E / parts).
+    const std::uint32_t V = parts * npad;
+    std::vector<std::vector<std::uint32_t>> vl(V);
     SicHost s;
-    const std::uint32_t slices = (N + 31) / 32;
+    for (std::uint32_t t = 0; t < N; ++t) {
+        std::uint32_t E = 0;
+        for (std::uint32_t x : lists[t]) E += x & 0xFFu;
+        s.max_edges = std::max(s.max_edges, E);
+        std::uint32_t done = 0, p = 0;
+        for (std::uint32_t x : lists[t]) {
+            std::uint32_t m = x & 0xFFu;
+            const std::uint32_t a = x >> 8;
+            while (m > 0) {
+                // end (exclusive, in edges) of part p
+                std::uint32_t end = static_cast<std::uint32_t>(
+                    (static_cast<std::uint64_t>(p + 1) * E) / parts);
+                while (done >= end && p + 1 < parts) {
+                    ++p;
+                    end = static_cast<std::uint32_t>((static_cast<std::uint64_t>(p + 1) * E) / parts);
+                }
+                const std::uint32_t take = std::min(m, end - done);
+                vl[p * npad + t].push_back((a << 8) | take);
+                done += take;
+                m -= take;
+            }
+        }
+    }
+    const std::uint32_t slices = V / 32;
     s.soff.assign(slices + 1, 0);
     for (std::uint32_t sl = 0; sl < slices; ++sl) {
         std::size_t len = 0;
-        for (std::uint32_t t = sl * 32; t < std::min(N, sl * 32 + 32); ++t)
-            len = std::max(len, lists[t].size());
+        for (std::uint32_t v = sl * 32; v < sl * 32 + 32; ++v) len = std::max(len, vl[v].size());
         s.soff[sl + 1] = s.soff[sl] + static_cast<std::uint32_t>(len * 32);
     }
     s.ent.assign(std::max<std::uint32_t>(s.soff[slices], 1), 0u);
-    for (std::uint32_t t = 0; t < N; ++t) {
-        const std::uint32_t sl = t / 32, lane = t % 32;
-        for (std::size_t q = 0; q < lists[t].size(); ++q)
-            s.ent[s.soff[sl] + q * 32 + lane] = lists[t][q];
+    for (std::uint32_t v = 0; v < V; ++v) {
+        const std::uint32_t sl = v / 32, lane = v % 32;
+        for (std::size_t q = 0; q < vl[v].size(); ++q)
+            s.ent[s.soff[sl] + q * 32 + lane] = vl[v][q];
     }
     return s;
 }
@@ -286,7 +328,9 @@ int Engine::footprint(const asg_network_desc& d, int chunk_steps, std::uint64_t*
     const std::uint64_t words = (Ee + Ei + Ea) / 32 + 2 * N + NA;  // upper bound
     b += (Ee + Ei + Ea) * 9 + (N * 3 + NA) * 8;       // out lists, bit positions, word bases
     b += slots * words * (4 + 32 * 8) + slots * (2 * N + NA) * 8;  // bits, values, summaries
+    b += slots * (2 * N + NA) * (4 + kListCap * 12);                // counters, short lists
     b += Es * 4 + N * 8 + slots * NA * 8 + 2 * N * 8;  // SIC (upper bound), factors, values
+    b += (N + 32) * (kMaxSicParts * 8 + 2 * kMaxSicParts * 8);  // part cuts, partial sums
     b += 256 * 64;                                     // alignment slack
     (void)chunk_steps;
     *bytes = b;
@@ -340,10 +384,12 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     // Deferred push needs both spike delays >= 2 steps (the push of step s
     // runs in step s+1 and must land before step s+d reads it).
     D.deferred_push = (cfg.push_mode != 1 && d.d_e_steps >= 2 && d.d_i_steps >= 2) ? 1 : 0;
-    // Enough push threads for a synchronous burst (every edge of a large
-    // fraction of the network in one step), at most two blocks per SM.
+    // One push block per kPushCells neurons, at most two per SM: the grid
+    // of a step (push, SIC parts, neurons, astrocytes) should fit the GPU in
+    // one wave; a burst is spread over the blocks' threads by striding.
     D.push_blocks = static_cast<std::int32_t>(std::min<std::uint32_t>(
-        2u * static_cast<std::uint32_t>(sms), std::max<std::uint32_t>(1, (N + 63) / 64)));
+        2u * static_cast<std::uint32_t>(sms),
+        std::max<std::uint32_t>(1, (N + kPushCells - 1) / kPushCells)));
     D.seed = d.seed;
     D.dt = d.dt;
     const double h = d.dt / static_cast<double>(d.substeps);
@@ -400,7 +446,18 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     InRingHost rex = make_in_ring(NE, rs_of(d.exc_primary), d.exc_primary.target, N);
     InRingHost rin = make_in_ring(NI, rs_of(d.inh_primary), d.inh_primary.target, N);
     InRingHost ras = make_in_ring(NE, rs_of(d.neuron_astro), d.neuron_astro.target, NA);
-    SicHost sic = make_sic(NA, rs_of(d.astro_neuron), d.astro_neuron.target, N);
+    // SIC parts: about kSicEdgesPerPart edges each, at most d_a2n - 1 (the
+    // first part of arrival step A runs at step A - P and reads the factors
+    // of step A - d_a2n, written by an earlier launch).
+    D.sic_npad = (N + 31) / 32 * 32;
+    D.sic_parts = 1;
+    if (!D.fused_sic) {
+        const std::uint32_t mx = sic_max_edges(NA, rs_of(d.astro_neuron), d.astro_neuron.target, N);
+        const int want = static_cast<int>((mx + kSicEdgesPerPart - 1) / kSicEdgesPerPart);
+        D.sic_parts = std::max(1, std::min({want, kMaxSicParts, D.d_a2n - 1}));
+    }
+    SicHost sic = make_sic(NA, rs_of(d.astro_neuron), d.astro_neuron.target, N,
+                           static_cast<std::uint32_t>(D.sic_parts), D.sic_npad);
 
     // Initial state (reference defaults where not given).
     std::vector<double> V0, Ca0, IP30, h0, stp_x(N, 1.0), stp_u(N, d.stp.U), stp_t(N, -1e12);
@@ -465,6 +522,10 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
         const std::size_t W = std::max<std::uint32_t>(H.words, 1);
         add_seg(R.wbase, H.wbase.size() * 4, H.wbase.data());
         add_seg(R.edge, H.edge.size() * 8, H.edge.data());
+        const std::size_t T = std::max<std::uint32_t>(n_t, 1);
+        add_seg(R.cnt, S * T * 4, nullptr);
+        add_seg(R.lbit, S * T * kListCap * 4, nullptr);
+        add_seg(R.lval, S * T * kListCap * 8, nullptr);
         add_seg(R.bits, S * W * 4, nullptr);
         add_seg(R.sum, S * std::max<std::uint32_t>(n_t, 1) * 8, nullptr);
         add_seg(R.vals, S * W * 32 * 8, nullptr);
@@ -481,6 +542,8 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     add_seg(D.sic_soff, sic.soff.size() * 4, sic.soff.data());
     add_seg(D.sic_ent, sic.ent.size() * 4, sic.ent.data());
     add_seg(D.fac, S * std::max<std::size_t>(a8, 8), nullptr);
+    add_seg(D.sic_part,
+            2 * static_cast<std::size_t>(std::max(D.sic_parts - 1, 1)) * D.sic_npad * 8, nullptr);
     add_seg(D.sic_val, 2 * std::max<std::size_t>(n8, 8), nullptr);
 
     std::size_t total = 0;
@@ -620,7 +683,9 @@ int Engine::rebuild() {
                                         static_cast<std::uint32_t>(pb), 0});
                 continue;
             }
-            const std::uint32_t n = r == kRoleAstro ? D.NA : D.N;
+            const std::uint32_t n = r == kRoleAstro ? D.NA
+                                    : r == kRoleSic ? static_cast<std::uint32_t>(D.sic_parts) * D.sic_npad
+                                                    : D.N;
             for (std::uint32_t f = 0; f < n; f += B)
                 work.push_back(Work{static_cast<std::uint32_t>(s), r, 0, f,
                                     std::min<std::uint32_t>(B, n - f)});

@@ -17,16 +17,22 @@
 // Exact, reproducible arrivals without floating-point atomics
 // ----------------------------------------------------------
 // The reference sums each ring entry sequentially in ascending source order
-// (network.cpp:249-279).  Here every target owns one bit per incoming edge,
-// its in-edges sorted by (source, position in the source's row), in bitmap
-// words of its own.  A spiking source writes the value w*x*u of each out-edge
-// at that edge's bit position, sets the bit (integer atomicOr, no return
-// value), and sets the target's summary bit for the word group holding it
-// (64-bit summary per target and slot).  The target, when the slot arrives,
-// visits only the non-empty words its summary names, walks their set bits
-// in ascending order and adds the values left to right: the reference's IEEE
-// operations in the reference's order, hence bitwise equal, for any number
-// of coincident spikes.  Reading clears the summary and the words it used.
+// (network.cpp:249-279).  Here every target numbers its incoming edges in
+// (source, position in the source's row) order; an arrival is identified by
+// that number (its "bit").  A push takes a ticket from the target's per-slot
+// arrival counter (integer atomicAdd).  Tickets 0..kListCap-1 store (bit,
+// value) in the target's short list for the slot; later tickets store the
+// value at the bit's position, set the bit in the target's bitmap words
+// (integer atomicOr, no return value) and set the target's summary bit for
+// the word group holding it (64-bit summary per target and slot).  The
+// target, when the slot arrives, reads its counter; for up to kListCap
+// arrivals it loads the list in one batch and sorts it by bit; beyond that it
+// also visits the non-empty words its summary names, walking their set bits
+// in ascending order and merging them with the sorted list.  Either way the
+// values are added left to right in ascending bit order: the reference's
+// IEEE operations in the reference's order, hence bitwise equal, for any
+// number of coincident spikes and any interleaving of the pushes.  Reading
+// clears the counter, the summary and the words it used.
 //
 // STP: the reference keeps x, u, t_last per edge, but all edges of a source
 // start equal (network.cpp:43-52) and are updated together on each spike of
@@ -37,7 +43,13 @@
 // ascending astrocyte order (network.cpp:281-299).  A target's edges from one
 // astrocyte all add the same value, so its list is stored compressed as
 // (astrocyte, multiplicity) pairs in ascending astrocyte order and summed
-// sequentially -- same operations, far fewer bytes.  Layout: sliced ELL with
+// sequentially -- same operations, far fewer bytes.  The sum is one chain
+// of dependent additions (hundreds per target), so when the SIC delay
+// allows it the chain is cut into P consecutive parts of about equal edge
+// count, computed on P consecutive steps by P threads: the part-p thread of
+// step s continues, for the arrival step s+P-p, the partial sum the
+// part-(p-1) thread left at step s-1.  Every addition is the reference's, in
+// its order; a step's longest chain is 1/P of a target's.  Layout: sliced ELL with
 // slices of 32 targets (one warp), entries packed as astro << 8 | mult.
 #pragma once
 
@@ -58,12 +70,18 @@ struct Work {
 };
 
 // Incoming-edge structure of one arrival ring (transpose of a source CSR).
+constexpr int kListCap = 4;      // arrivals per (slot, target) held in the short list
+constexpr int kMaxSicParts = 8;  // most parts a target's SIC chain is cut into
+
 struct InRing {
     const std::uint32_t* wbase;   // [n_targets+1] first bitmap word of each target
     // [E] per OUT-edge (source CSR order): bit index | target << 32 | summary
     // bit << 58 -- one 8-byte load gives everything a push needs.
     const unsigned long long* edge;
-    std::uint32_t* bits;          // [slots][words] arrival bitmaps
+    std::uint32_t* cnt;           // [slots][n_targets] arrivals pushed into the slot
+    std::uint32_t* lbit;          // [slots][n_targets][kListCap] bits of the first arrivals
+    double* lval;                 // [slots][n_targets][kListCap] their values
+    std::uint32_t* bits;          // [slots][words] bitmaps of the later arrivals
     unsigned long long* sum;      // [slots][n_targets] non-empty word groups
     double* vals;                 // [slots][words*32] value at each set bit
     std::uint32_t words;          // total bitmap words of one slot
@@ -117,10 +135,14 @@ struct InstDev {
     unsigned long long* spk_packed;    // [3]: count << 40 | edges
     std::uint32_t* spk_meta;           // [3][N][4]: source, edge offset, row0 start, row0 length
     double* spk_val;                   // [3][N][2]: exc or inh set value, n2a value
-    // SIC: sliced ELL over targets, factors per emission slot, split values
-    const std::uint32_t* sic_soff;  // [n_slices+1] entry offset of each 32-target slice
+    // SIC: sliced ELL over virtual targets v = part * sic_npad + target,
+    // factors per emission slot, partial sums between parts, final values
+    std::int32_t sic_parts;         // P (1 when the delay is too short to split)
+    std::uint32_t sic_npad;         // N rounded up to a multiple of 32
+    const std::uint32_t* sic_soff;  // [P*sic_npad/32+1] entry offset of each 32-target slice
     const std::uint32_t* sic_ent;   // astro << 8 | mult
     double* fac;                    // [slots][NA]
+    double* sic_part;               // [2][P-1][sic_npad] partial sums, by step parity
     double* sic_val;                // [2][N]
     // outputs (host-mapped memory)
     unsigned long long* spike_log;  // (step << 32) | source

@@ -2,6 +2,18 @@
 // asg_engine.cuh).  Compiled with -fmad=false: every floating-point
 // expression is evaluated as separate IEEE operations in the reference's
 // order (neuron.cpp:101-250, astrocyte.cpp:233-329, network.cpp:230-355).
+//
+// Latency, not bandwidth, bounds a step of a network of this size: each
+// role is a short chain of dependent memory round trips and FP64 operations,
+// and a step ends with its slowest thread.  So every role (1) reads what the
+// previous step cannot have changed (per-cell constants, CSR rows, SIC lists)
+// BEFORE waiting on the previous step's grid, (2) then issues every load of
+// the step's inputs at once, (3) reads its arrivals with one more batch of
+// loads in the common case of a few arrivals per target, and (4) keeps rare
+// paths (noise, the large-lambda Poisson branch, many-arrival merges, the
+// in-block push, the fused SIC) out of line so the instruction stream of the
+// common path stays small.  The per-step slot and modulo arithmetic is done
+// once per block, also before the wait.
 
 #include <cuda_runtime.h>
 
@@ -12,6 +24,60 @@ namespace asg {
 namespace {
 
 constexpr int kMaxBlock = 512;
+constexpr std::uint32_t kNoBit = 0xFFFFFFFFu;
+constexpr int kSicBatch = 8;  // SIC list entries loaded per batch
+
+__device__ __forceinline__ void grid_dep_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Everything about the current step that is the same for a whole block.
+struct StepInfo {
+    std::int64_t step;
+    std::uint32_t slot;        // ring slot read this step: step % slots
+    std::uint32_t fslot;       // factor slot of the SIC arriving now (fused SIC)
+    // SIC role: part p works on arrival step+P-p; bit p of sic_due says
+    // that arrival takes SIC, sic_slot[p] is its factor slot
+    std::uint32_t sic_due;
+    std::uint32_t sic_slot[kMaxSicParts];
+    std::uint32_t push_e, push_i;          // deferred push of step-1's spikes
+    std::uint32_t now_e, now_i;            // in-block push of this step's spikes
+    std::uint32_t ls, ls_prev, ls_next;    // spike-list slots of step, step-1, step+1
+    std::uint32_t rec_row;
+    std::uint64_t noise_e, noise_i, noise_a;  // noise draw indices
+    std::int32_t sic_now, fac_now, rec_now;
+};
+
+__device__ void make_step_info(const InstDev& I, std::int64_t step, StepInfo& S) {
+    const std::int64_t slots = I.slots;
+    S.step = step;
+    S.slot = static_cast<std::uint32_t>(step % slots);
+    const std::int64_t se = step - I.d_a2n;
+    S.sic_now = se >= 0 && se % I.sic_interval == 0;
+    S.fslot = se >= 0 ? static_cast<std::uint32_t>(se % slots) : 0u;
+    S.sic_due = 0;
+    for (int p = 0; p < I.sic_parts; ++p) {
+        const std::int64_t sp = step + I.sic_parts - p - I.d_a2n;
+        const bool due = sp >= 0 && sp % I.sic_interval == 0;
+        S.sic_due |= due ? (1u << p) : 0u;
+        S.sic_slot[p] = due ? static_cast<std::uint32_t>(sp % slots) : 0u;
+    }
+    S.push_e = static_cast<std::uint32_t>((step - 1 + I.d_e) % slots);
+    S.push_i = static_cast<std::uint32_t>((step - 1 + I.d_i) % slots);
+    S.now_e = static_cast<std::uint32_t>((step + I.d_e) % slots);
+    S.now_i = static_cast<std::uint32_t>((step + I.d_i) % slots);
+    S.ls = static_cast<std::uint32_t>(step % 3);
+    S.ls_prev = static_cast<std::uint32_t>((step + 2) % 3);
+    S.ls_next = static_cast<std::uint32_t>((step + 1) % 3);
+    S.fac_now = step % I.sic_interval == 0;
+    S.rec_now = step >= I.rec_from && (step - I.rec_from) % I.rec_every == 0;
+    S.rec_row = S.rec_now ? static_cast<std::uint32_t>(((step - I.rec_from) / I.rec_every) %
+                                                       static_cast<std::int64_t>(I.rec_rows))
+                          : 0u;
+    S.noise_e = static_cast<std::uint64_t>(step / I.pe.steps_per_noise);
+    S.noise_i = static_cast<std::uint64_t>(step / I.pi.steps_per_noise);
+    S.noise_a = static_cast<std::uint64_t>(step / I.a_steps_per_noise);
+}
 
 // Routes one arrival the way NeuronPopulation::add_synaptic_input does
 // (neuron.cpp:77-83): positive weights to the excitatory input, negative
@@ -24,20 +90,69 @@ __device__ __forceinline__ void add_syn(double v, double& exc_in, double& inh_in
     }
 }
 
-// Ordered sum of one target's arrivals in `slot` (see asg_engine.cuh), given
-// the summary word already read (and cleared) by the caller.  Loads are
-// issued in batches of independent requests -- up to 8 bitmap words, then up
-// to 8 values -- so a target with several arrivals pays a few memory round
-// trips, not one per arrival; the additions stay in ascending bit order.
-// kSubtract selects ring_inh's `-=` accumulation (network.cpp:271-275).
-template <bool kSubtract>
-__device__ __forceinline__ double ring_gather(const InRing& R, int slot, std::uint32_t t,
-                                              unsigned long long groups) {
+// ------------------------------------------------------------- arrivals
+
+// One batch of loads: the (bit, value) pairs of the first kListCap arrivals
+// of (slot, target) `ts`.
+struct ShortList {
+    uint4 bit;
+    double2 v01, v23;
+};
+
+__device__ __forceinline__ ShortList load_list(const InRing& R, std::size_t ts) {
+    ShortList l;
+    l.bit = __ldcg(reinterpret_cast<const uint4*>(R.lbit) + ts);
+    l.v01 = __ldcg(reinterpret_cast<const double2*>(R.lval) + 2 * ts);
+    l.v23 = __ldcg(reinterpret_cast<const double2*>(R.lval) + 2 * ts + 1);
+    return l;
+}
+
+__device__ __forceinline__ void order2(std::uint32_t& ba, double& va, std::uint32_t& bb,
+                                       double& vb) {
+    const bool swap = bb < ba;
+    const std::uint32_t b = swap ? bb : ba;
+    const double v = swap ? vb : va;
+    bb = swap ? ba : bb;
+    vb = swap ? va : vb;
+    ba = b;
+    va = v;
+}
+
+__device__ __forceinline__ double accumulate(double acc, double v, bool sub) {
+    return sub ? acc - v : acc + v;
+}
+
+// More than kListCap arrivals: the first kListCap (sorted, l0 < l1 < l2 <
+// l3) are merged in bit order with the later ones, which sit in the
+// target's bitmap words (visited through the summary).  Bitmap loads go out
+// in batches -- up to 8 words, then up to 8 values -- so a burst costs a few
+// round trips, not one per arrival.  Clears the summary and the words.
+__device__ __noinline__ double merge_overflow(const InRing& R, std::uint32_t slot,
+                                              std::uint32_t t, bool sub, std::uint32_t l0,
+                                              std::uint32_t l1, std::uint32_t l2,
+                                              std::uint32_t l3, double v0, double v1, double v2,
+                                              double v3) {
+    unsigned long long* sp = R.sum + static_cast<std::size_t>(slot) * R.n_targets + t;
+    unsigned long long groups = __ldcg(sp);
+    *sp = 0;
     std::uint32_t* bits = R.bits + static_cast<std::size_t>(slot) * R.words;
     const double* vals = R.vals + static_cast<std::size_t>(slot) * R.words * 32;
     const std::uint32_t w0 = R.wbase[t], nw = R.wbase[t + 1] - w0;
     const std::uint32_t G = (nw + 63) >> 6;  // words per summary bit
     double acc = 0.0;
+    // Adds the list entries that precede `bit`.
+    auto drain = [&](std::uint32_t bit) {
+        while (l0 < bit) {
+            acc = accumulate(acc, v0, sub);
+            l0 = l1;
+            v0 = v1;
+            l1 = l2;
+            v1 = v2;
+            l2 = l3;
+            v2 = v3;
+            l3 = kNoBit;
+        }
+    };
     std::uint32_t idx[8];
     int n = 0;
     auto flush = [&]() {
@@ -47,24 +162,12 @@ __device__ __forceinline__ double ring_gather(const InRing& R, int slot, std::ui
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             if (k < n) {
-                if (kSubtract) {
-                    acc -= v[k];
-                } else {
-                    acc += v[k];
-                }
+                drain(idx[k]);
+                acc = accumulate(acc, v[k], sub);
             }
         }
         n = 0;
     };
-    auto take_word = [&](std::uint32_t q, std::uint32_t word) {
-        while (word != 0) {
-            const int b = __ffs(word) - 1;
-            word &= word - 1;
-            idx[n++] = q * 32 + b;
-            if (n == 8) flush();
-        }
-    };
-    // Word groups in ascending order, up to 8 words loaded at once.
     std::uint32_t q[8], wv[8];
     std::uint32_t cur = 0, cur_end = 0;  // words [cur, cur_end) of the open group
     bool open = false;
@@ -91,131 +194,245 @@ __device__ __forceinline__ double ring_gather(const InRing& R, int slot, std::ui
 #pragma unroll
         for (int k = 0; k < 8; ++k)
             if (k < nq && wv[k] != 0) bits[q[k]] = 0;
-        for (int k = 0; k < nq; ++k) take_word(q[k], wv[k]);
-    }
-    flush();
-    return acc;
-}
-
-// Sequential SIC sum of target t from the factors of emission slot fslot
-// (network.cpp:281-299 order: ascending astrocyte, one add per edge).  The
-// list entries and their factors are fetched 8 at a time with independent
-// loads before the dependent additions.
-__device__ __forceinline__ double sic_sum(const InstDev& I, std::uint32_t t, int fslot,
-                                          unsigned long long& edges) {
-    const std::uint32_t slice = t >> 5, lane = t & 31;
-    const std::uint32_t o0 = I.sic_soff[slice], o1 = I.sic_soff[slice + 1];
-    const std::uint32_t len = (o1 - o0) >> 5;
-    const double* fac = I.fac + static_cast<std::size_t>(fslot) * I.NA;
-    double acc = 0.0;
-    for (std::uint32_t b0 = 0; b0 < len; b0 += 8) {
-        std::uint32_t e[8];
-        double f[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) e[k] = b0 + k < len ? __ldg(I.sic_ent + o0 + (b0 + k) * 32 + lane) : 0u;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) f[k] = (e[k] & 0xFFu) ? __ldcg(fac + (e[k] >> 8)) : 0.0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const std::uint32_t m = e[k] & 0xFFu;
-            if (m == 0) return acc;  // padding ends the list
-            if (f[k] == 0.0) continue;
-            const double c = I.w_a2n * f[k];
-            for (std::uint32_t r = 0; r < m; ++r) acc += c;
-            edges += m;
+        for (int k = 0; k < nq; ++k) {
+            std::uint32_t word = wv[k];
+            while (word != 0) {
+                const int b = __ffs(word) - 1;
+                word &= word - 1;
+                idx[n++] = q[k] * 32 + b;
+                if (n == 8) flush();
+            }
         }
     }
+    flush();
+    drain(kNoBit);
     return acc;
 }
 
-// One arrival: value at the edge's bit, the bit, the target's summary bit.
-__device__ __forceinline__ void push_edge(const InRing& R, int slot, unsigned long long pe,
-                                          double value) {
+// Ordered sum of the `n` (>= 1) arrivals of target t in `slot`, given its
+// short list.  kSubtract selects ring_inh's `-=` accumulation
+// (network.cpp:271-275).
+template <bool kSubtract>
+__device__ __forceinline__ double sum_arrivals(const InRing& R, std::uint32_t slot,
+                                               std::uint32_t t, std::uint32_t n,
+                                               const ShortList& l) {
+    std::uint32_t b0 = l.bit.x, b1 = n > 1 ? l.bit.y : kNoBit, b2 = n > 2 ? l.bit.z : kNoBit,
+                  b3 = n > 3 ? l.bit.w : kNoBit;
+    double v0 = l.v01.x, v1 = l.v01.y, v2 = l.v23.x, v3 = l.v23.y;
+    order2(b0, v0, b1, v1);
+    order2(b2, v2, b3, v3);
+    order2(b0, v0, b2, v2);
+    order2(b1, v1, b3, v3);
+    order2(b1, v1, b2, v2);
+    if (n > static_cast<std::uint32_t>(kListCap))
+        return merge_overflow(R, slot, t, kSubtract, b0, b1, b2, b3, v0, v1, v2, v3);
+    double acc = accumulate(0.0, v0, kSubtract);
+    if (n > 1) acc = accumulate(acc, v1, kSubtract);
+    if (n > 2) acc = accumulate(acc, v2, kSubtract);
+    if (n > 3) acc = accumulate(acc, v3, kSubtract);
+    return acc;
+}
+
+// One arrival on the edge with packed word `pe` (bit | target << 32 |
+// summary bit << 58): a ticket from the target's counter decides between
+// the short list and the bitmap.
+__device__ __forceinline__ void push_edge(const InRing& R, std::uint32_t slot,
+                                          unsigned long long pe, double value) {
     const std::uint32_t b = static_cast<std::uint32_t>(pe);
     const std::uint32_t t = static_cast<std::uint32_t>(pe >> 32) & 0x3FFFFFFu;
-    const std::uint32_t g = static_cast<std::uint32_t>(pe >> 58);
-    R.vals[static_cast<std::size_t>(slot) * R.words * 32 + b] = value;
-    atomicOr(R.bits + static_cast<std::size_t>(slot) * R.words + (b >> 5), 1u << (b & 31));
-    atomicOr(R.sum + static_cast<std::size_t>(slot) * R.n_targets + t, 1ull << g);
+    const std::size_t ts = static_cast<std::size_t>(slot) * R.n_targets + t;
+    const std::uint32_t k = atomicAdd(R.cnt + ts, 1u);
+    if (k < static_cast<std::uint32_t>(kListCap)) {
+        R.lbit[ts * kListCap + k] = b;
+        R.lval[ts * kListCap + k] = value;
+    } else {
+        const std::uint32_t g = static_cast<std::uint32_t>(pe >> 58);
+        R.vals[static_cast<std::size_t>(slot) * R.words * 32 + b] = value;
+        atomicOr(R.bits + static_cast<std::size_t>(slot) * R.words + (b >> 5), 1u << (b & 31));
+        atomicOr(R.sum + ts, 1ull << g);
+    }
 }
 
 // Writes `value` at every out-edge of `row` (in-block push, used when a
 // spike delay is a single step).
-__device__ __forceinline__ void push_row(const std::uint32_t* rs, const InRing& R,
-                                         std::uint32_t row, int slot, double value) {
+__device__ __noinline__ void push_row(const std::uint32_t* rs, const InRing& R, std::uint32_t row,
+                                      std::uint32_t slot, double value) {
     const std::uint32_t e1 = rs[row + 1];
 #pragma unroll 4
     for (std::uint32_t e = rs[row] + threadIdx.x; e < e1; e += blockDim.x)
         push_edge(R, slot, __ldg(R.edge + e), value);
 }
 
-__device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step) {
+// ---------------------------------------------------------------- SIC
+
+// Sequential SIC sum from the factors of emission slot fslot, continuing
+// `acc` (network.cpp:281-299 order: ascending astrocyte, one add of
+// w_a2n * factor per edge).  `e` holds the first kSicBatch list entries
+// (loaded by the caller); the factors of a batch are fetched with
+// independent loads before its additions.
+__device__ __forceinline__ double sic_sum(const InstDev& I, std::uint32_t o0, std::uint32_t len,
+                                          std::uint32_t (&e)[kSicBatch], std::uint32_t fslot,
+                                          double acc, unsigned long long& edges) {
+    const double* fac = I.fac + static_cast<std::size_t>(fslot) * I.NA;
+    for (std::uint32_t b0 = 0;; b0 += kSicBatch) {
+        double f[kSicBatch];
+#pragma unroll
+        for (int k = 0; k < kSicBatch; ++k) f[k] = (e[k] & 0xFFu) ? __ldcg(fac + (e[k] >> 8)) : 0.0;
+        bool done = false;
+#pragma unroll
+        for (int k = 0; k < kSicBatch; ++k) {
+            const std::uint32_t m = e[k] & 0xFFu;
+            if (m == 0) {
+                done = true;  // padding ends the list
+                break;
+            }
+            if (f[k] == 0.0) continue;
+            const double c = I.w_a2n * f[k];
+            for (std::uint32_t r = 0; r < m; ++r) acc += c;
+            edges += m;
+        }
+        if (done || b0 + kSicBatch >= len) break;
+#pragma unroll
+        for (int k = 0; k < kSicBatch; ++k) {
+            const std::uint32_t j = b0 + kSicBatch + k;
+            e[k] = j < len ? __ldg(I.sic_ent + o0 + j * 32) : 0u;
+        }
+    }
+    return acc;
+}
+
+// First batch of a target's SIC list entries (static data).  o0 is the
+// target's first entry; entries of one target are 32 apart (sliced ELL).
+__device__ __forceinline__ void sic_prefetch(const InstDev& I, std::uint32_t t, std::uint32_t& o0,
+                                             std::uint32_t& len,
+                                             std::uint32_t (&e)[kSicBatch]) {
+    const std::uint32_t slice = t >> 5;
+    const std::uint32_t s0 = I.sic_soff[slice], s1 = I.sic_soff[slice + 1];
+    o0 = s0 + (t & 31);
+    len = (s1 - s0) >> 5;
+#pragma unroll
+    for (int k = 0; k < kSicBatch; ++k)
+        e[k] = static_cast<std::uint32_t>(k) < len ? __ldg(I.sic_ent + o0 + k * 32) : 0u;
+}
+
+// SIC of a neuron summed by its own thread (fused mode, SIC delay of one step).
+__device__ __noinline__ double fused_sic(const InstDev& I, std::uint32_t c, std::uint32_t fslot) {
+    std::uint32_t o0, len, e[kSicBatch];
+    sic_prefetch(I, c, o0, len, e);
+    unsigned long long edges = 0;
+    const double v = sic_sum(I, o0, len, e, fslot, 0.0, edges);
+    if (edges) atomicAdd(I.counters + 1, edges);
+    return v;
+}
+
+// ---------------------------------------------------------------- noise
+
+// Box-Muller draws, out of line (log, sqrt and cos are sizeable code and
+// most configurations run without noise).
+__device__ __noinline__ double normal_first_at(std::uint64_t seed, std::uint64_t stream) {
+    Draws r(seed, stream);
+    return r.normal_first();
+}
+
+__device__ __noinline__ double normal_clamped_at(std::uint64_t seed, std::uint64_t stream) {
+    return normal_clamped(seed, stream);
+}
+
+// --------------------------------------------------------------- roles
+
+template <bool kPdl>
+__device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     __shared__ std::uint32_t s_spk[kMaxBlock];
     __shared__ double s_val[2 * kMaxBlock];
     __shared__ int s_nspk;
     if (threadIdx.x == 0) s_nspk = 0;
-    __syncthreads();
 
     const std::uint32_t c = wk.first + threadIdx.x;
-    if (threadIdx.x < wk.count) {
-        const bool exc = c < I.NE;
-        const NeuronK& P = exc ? I.pe : I.pi;
-        const int slot = static_cast<int>(step % I.slots);
+    const bool active = threadIdx.x < wk.count;
+    const bool exc = c < I.NE;
+    // Written before the chunk started: read before waiting on the
+    // previous step.
+    double Vr = 0.0, bc = 0.0;
+    std::uint32_t r0 = 0, len0 = 0, len1 = 0;
+    if (active) {
+        Vr = I.V_reset[c];
+        bc = I.b[c];
+        if (exc) {
+            r0 = I.exc_rs[c];
+            len0 = I.exc_rs[c + 1] - r0;
+            len1 = I.n2a_rs[c + 1] - I.n2a_rs[c];
+        } else {
+            r0 = I.inh_rs[c - I.NE];
+            len0 = I.inh_rs[c - I.NE + 1] - r0;
+        }
+    }
+    if (kPdl) grid_dep_wait();
+    __syncthreads();
+    const std::int64_t step = S.step;
+    if (step >= I.end_step) return;
 
-        // Issue every independent load of this cell before any store.
-        const std::size_t so = static_cast<std::size_t>(slot);
-        unsigned long long* sp_ex = I.ring_ex.sum + so * I.ring_ex.n_targets + c;
-        unsigned long long* sp_in = I.ring_in.sum + so * I.ring_in.n_targets + c;
-        const unsigned long long g_ex = __ldcg(sp_ex), g_in = __ldcg(sp_in);
-        const std::int64_t se = step - I.d_a2n;
-        const bool sic_due = se >= 0 && se % I.sic_interval == 0;
+    if (active) {
+        const NeuronK& P = exc ? I.pe : I.pi;
+        const std::uint32_t slot = S.slot;
+
+        // Every input of the step in one batch of independent loads.
+        const std::size_t ts_ex = static_cast<std::size_t>(slot) * I.ring_ex.n_targets + c;
+        const std::size_t ts_in = static_cast<std::size_t>(slot) * I.ring_in.n_targets + c;
+        const std::uint32_t n_ex = __ldcg(I.ring_ex.cnt + ts_ex);
+        const std::uint32_t n_in = __ldcg(I.ring_in.cnt + ts_in);
+        const bool sic_due = S.sic_now != 0;
         double Isic = (sic_due && !I.fused_sic)
                           ? __ldcg(I.sic_val + static_cast<std::size_t>(step & 1) * I.N + c)
                           : I.Isic[c];
         double V = I.V[c], w = I.w[c], gex = I.gex[c], gin = I.gin[c];
         double dgex = I.dgex[c], dgin = I.dgin[c];
         int refr = I.refr[c];
-        const double Vr = I.V_reset[c], bc = I.b[c];
+        double sx = 1.0, su = 1.0, st = 0.0;
+        if (I.stp_on) {
+            sx = I.stp_x[c];
+            su = I.stp_u[c];
+            st = I.stp_t[c];
+        }
 
-        // apply_arrivals (network.cpp:301-338)
+        // Draws need no memory: they overlap the loads above.
+        int ev = 0;
+        if (P.poiss_rate > 0.0) {
+            Draws r(I.seed ^ kSaltNeuronPoisson,
+                    static_cast<std::uint64_t>(step) * kStreamStride + c);
+            ev = r.poisson(P.lambda, P.knuth_limit);
+        }
+        double z = 0.0;
+        if (P.noise_std > 0.0) {
+            const std::uint64_t idx = exc ? S.noise_e : S.noise_i;
+            z = P.independent_noise
+                    ? normal_first_at(I.seed ^ kSaltNeuronNoise, idx * kNoiseStride + c)
+                    : normal_first_at(I.seed ^ (exc ? kSaltSharedExc : kSaltSharedInh), idx);
+        }
+
+        // apply_arrivals (network.cpp:301-338): both short lists in one batch.
+        ShortList lex{}, lin{};
+        if (n_ex) lex = load_list(I.ring_ex, ts_ex);
+        if (n_in) lin = load_list(I.ring_in, ts_in);
         double exc_in = 0.0, inh_in = 0.0;
-        if (g_ex != 0) {
-            *sp_ex = 0;
-            const double ex = ring_gather<false>(I.ring_ex, slot, c, g_ex);
+        if (n_ex) {
+            I.ring_ex.cnt[ts_ex] = 0;
+            const double ex = sum_arrivals<false>(I.ring_ex, slot, c, n_ex, lex);
             if (ex != 0.0) add_syn(ex, exc_in, inh_in);
         }
-        if (g_in != 0) {
-            *sp_in = 0;
-            const double in = ring_gather<true>(I.ring_in, slot, c, g_in);
+        if (n_in) {
+            I.ring_in.cnt[ts_in] = 0;
+            const double in = sum_arrivals<true>(I.ring_in, slot, c, n_in, lin);
             if (in != 0.0) add_syn(-in, exc_in, inh_in);
         }
         if (sic_due) {
-            if (I.fused_sic) {
-                unsigned long long edges = 0;
-                Isic = sic_sum(I, c, static_cast<int>(se % I.slots), edges);
-                if (edges) atomicAdd(I.counters + 1, edges);
-            }
+            if (I.fused_sic) Isic = fused_sic(I, c, S.fslot);
             I.Isic[c] = Isic;
         }
 
         // Poisson drive and noise (neuron.cpp:228-248)
-        if (P.poiss_rate > 0.0) {
-            Draws r(I.seed ^ kSaltNeuronPoisson,
-                    static_cast<std::uint64_t>(step) * kStreamStride + c);
-            const int ev = r.poisson(P.lambda, P.knuth_limit);
-            if (ev > 0) exc_in += P.poiss_weight * static_cast<double>(ev);
-        }
+        if (ev > 0) exc_in += P.poiss_weight * static_cast<double>(ev);
         double Iext = Isic;
-        if (P.noise_std > 0.0) {
-            const std::uint64_t idx = static_cast<std::uint64_t>(step / P.steps_per_noise);
-            if (P.independent_noise) {
-                Draws r(I.seed ^ kSaltNeuronNoise, idx * kNoiseStride + c);
-                Iext += 0.0 + P.noise_std * r.normal_first();
-            } else {
-                Draws r(I.seed ^ (exc ? kSaltSharedExc : kSaltSharedInh), idx);
-                Iext += 0.0 + P.noise_std * r.normal_first();
-            }
-        }
+        if (P.noise_std > 0.0) Iext += 0.0 + P.noise_std * z;
 
         if (exc_in != 0.0) dgex += exc_in * P.psc_ex;
         if (inh_in != 0.0) dgin += inh_in * P.psc_in;
@@ -239,21 +456,21 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
                 const double gexm = 0.5 * (gex + gex1), ginm = 0.5 * (gin + gin1);
                 double sV = 0.0, sw = 0.0, xV = V, xw = w;
 #pragma unroll 1
-                for (int st = 0; st < 4; ++st) {
-                    const double ge = st == 0 ? gex : (st < 3 ? gexm : gex1);
-                    const double gi = st == 0 ? gin : (st < 3 ? ginm : gin1);
+                for (int stg = 0; stg < 4; ++stg) {
+                    const double ge = stg == 0 ? gex : (stg < 3 ? gexm : gex1);
+                    const double gi = stg == 0 ? gin : (stg < 3 ? ginm : gin1);
                     const AdexRates r = adex<true>(P, xV, xw, ge, gi, Iext);
-                    if (st == 0) {
+                    if (stg == 0) {
                         sV = r.V;
                         sw = r.w;
-                    } else if (st < 3) {
+                    } else if (stg < 3) {
                         sV = sV + 2.0 * r.V;
                         sw = sw + 2.0 * r.w;
                     } else {
                         sV = sV + r.V;
                         sw = sw + r.w;
                     }
-                    const double stp = st < 2 ? half_h : h;
+                    const double stp = stg < 2 ? half_h : h;
                     xV = V + stp * r.V;
                     xw = w + stp * r.w;
                 }
@@ -287,14 +504,12 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
             double x = 1.0, u = 1.0;
             if (I.stp_on) {
                 const double t_now = static_cast<double>(step) * I.dt;
-                const double d = t_now - I.stp_t[c];
+                const double d = t_now - st;
                 const double xd = exp(div_by(-d, I.tau_rec, I.inv_tau_rec));
                 const double ud =
                     I.tau_fac < 1e-10 ? 0.0 : exp(div_by(-d, I.tau_fac, I.inv_tau_fac));
-                x = I.stp_x[c];
-                u = I.stp_u[c];
-                x = 1.0 + (x - x * u - 1.0) * xd;
-                u = I.U + u * (1.0 - I.U) * ud;
+                x = 1.0 + (sx - sx * su - 1.0) * xd;
+                u = I.U + su * (1.0 - I.U) * ud;
                 I.stp_x[c] = x;
                 I.stp_u[c] = u;
                 I.stp_t[c] = t_now;
@@ -303,31 +518,16 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
                 exc ? (I.stp_on ? I.w_e * x * u : I.w_e) : (I.stp_on ? I.w_i * x * u : I.w_i);
             const double v1 = exc ? (I.stp_on ? I.w_n2a * x * u : I.w_n2a) : 0.0;
             if (I.deferred_push) {
-                const int ls = static_cast<int>(step % 3);
-                std::uint32_t r0, len0, len1;
-                if (exc) {
-                    r0 = I.exc_rs[c];
-                    len0 = I.exc_rs[c + 1] - r0;
-                    len1 = I.n2a_rs[c + 1] - I.n2a_rs[c];
-                } else {
-                    r0 = I.inh_rs[c - I.NE];
-                    len0 = I.inh_rs[c - I.NE + 1] - r0;
-                    len1 = 0;
-                }
                 const unsigned long long old = atomicAdd(
-                    I.spk_packed + ls, (1ull << 40) | static_cast<unsigned long long>(len0 + len1));
-                const std::size_t o = static_cast<std::size_t>(ls) * I.N + (old >> 40);
-                I.spk_meta[4 * o + 0] = c;
-                I.spk_meta[4 * o + 1] = static_cast<std::uint32_t>(old & 0xFFFFFFFFFFull);
-                I.spk_meta[4 * o + 2] = r0;
-                I.spk_meta[4 * o + 3] = len0;
-                I.spk_val[2 * o] = v0;
-                I.spk_val[2 * o + 1] = v1;
+                    I.spk_packed + S.ls,
+                    (1ull << 40) | static_cast<unsigned long long>(len0 + len1));
+                const std::size_t o = static_cast<std::size_t>(S.ls) * I.N + (old >> 40);
+                *reinterpret_cast<uint4*>(I.spk_meta + 4 * o) =
+                    make_uint4(c, static_cast<std::uint32_t>(old & 0xFFFFFFFFFFull), r0, len0);
+                *reinterpret_cast<double2*>(I.spk_val + 2 * o) = make_double2(v0, v1);
             } else {
                 s_val[threadIdx.x * 2 + 0] = v0;
                 s_val[threadIdx.x * 2 + 1] = v1;
-            }
-            if (!I.deferred_push) {
                 const int pos = atomicAdd(&s_nspk, 1);
                 s_spk[pos] = threadIdx.x;
             }
@@ -339,36 +539,31 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
                     atomicAdd(I.counters + 3, 1ULL);
                 }
             }
-            unsigned long long edges =
-                exc ? (I.exc_rs[c + 1] - I.exc_rs[c]) + (I.n2a_rs[c + 1] - I.n2a_rs[c])
-                    : (I.inh_rs[c - I.NE + 1] - I.inh_rs[c - I.NE]);
-            atomicAdd(I.counters + 0, edges);
+            atomicAdd(I.counters + 0, static_cast<unsigned long long>(len0 + len1));
             atomicAdd(I.counters + 2, 1ULL);
         }
 
-        if (I.rec_neuron_max > 0 && c < I.rec_neuron_max && step >= I.rec_from &&
-            (step - I.rec_from) % I.rec_every == 0) {
-            const std::size_t row =
-                static_cast<std::size_t>(((step - I.rec_from) / I.rec_every) % I.rec_rows);
+        if (I.rec_neuron_max > 0 && c < I.rec_neuron_max && S.rec_now) {
+            const std::size_t row = S.rec_row;
             I.rec_V[row * I.rec_neuron_max + c] = V;
             I.rec_Isic[row * I.rec_neuron_max + c] = Isic;
         }
     }
 
     // Push the out-edges of this block's spiking sources into the rings of
-    // their arrival steps (deliver_spikes, network.cpp:249-279).
+    // their arrival steps (deliver_spikes, network.cpp:249-279) when the
+    // push is not deferred to the next step.
+    if (I.deferred_push) return;
     __syncthreads();
     const int nspk = s_nspk;
     for (int q = 0; q < nspk; ++q) {
         const std::uint32_t lane = s_spk[q];
         const std::uint32_t j = wk.first + lane;
         if (j < I.NE) {
-            const int as = static_cast<int>((step + I.d_e) % I.slots);
-            push_row(I.exc_rs, I.ring_ex, j, as, s_val[2 * lane]);
-            push_row(I.n2a_rs, I.ring_as, j, as, s_val[2 * lane + 1]);
+            push_row(I.exc_rs, I.ring_ex, j, S.now_e, s_val[2 * lane]);
+            push_row(I.n2a_rs, I.ring_as, j, S.now_e, s_val[2 * lane + 1]);
         } else {
-            const int as = static_cast<int>((step + I.d_i) % I.slots);
-            push_row(I.inh_rs, I.ring_in, j - I.NE, as, s_val[2 * lane]);
+            push_row(I.inh_rs, I.ring_in, j - I.NE, S.now_i, s_val[2 * lane]);
         }
     }
 }
@@ -380,32 +575,36 @@ __device__ void neuron_role(const InstDev& I, const Work& wk, std::int64_t step)
 // list slot the next step appends to.
 constexpr int kPushBatch = 256;
 
-__device__ void push_role(const InstDev& I, const Work& wk, std::int64_t step) {
+template <bool kPdl>
+__device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     __shared__ std::uint32_t s_off[kPushBatch + 1], s_src[kPushBatch], s_r0[kPushBatch],
         s_len0[kPushBatch];
     __shared__ double s_v[2 * kPushBatch];
-    if (wk.first == 0 && threadIdx.x == 0) I.spk_packed[(step + 1) % 3] = 0;
+    if (kPdl) grid_dep_wait();
+    const std::int64_t step = S.step;
+    if (step >= I.end_step) return;
+    if (wk.first == 0 && threadIdx.x == 0) I.spk_packed[S.ls_next] = 0;
     if (step == 0) return;
-    const int ls = static_cast<int>((step - 1) % 3);
-    const unsigned long long packed = __ldcg(I.spk_packed + ls);
+    const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev);
     const std::uint32_t n = static_cast<std::uint32_t>(packed >> 40);
     const std::uint32_t total = static_cast<std::uint32_t>(packed & 0xFFFFFFFFFFull);
     const std::uint32_t stride = blockDim.x * I.push_blocks;
     const std::uint32_t gtid = wk.first * blockDim.x + threadIdx.x;
-    const int as_e = static_cast<int>((step - 1 + I.d_e) % I.slots);
-    const int as_i = static_cast<int>((step - 1 + I.d_i) % I.slots);
-    const std::size_t base = static_cast<std::size_t>(ls) * I.N;
+    const std::uint32_t as_e = S.push_e, as_i = S.push_i;
+    const std::size_t base = static_cast<std::size_t>(S.ls_prev) * I.N;
     for (std::uint32_t b0 = 0; b0 < n; b0 += kPushBatch) {
         const std::uint32_t nb = min(static_cast<std::uint32_t>(kPushBatch), n - b0);
         __syncthreads();
         for (std::uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
             const std::size_t o = base + b0 + i;
-            s_src[i] = __ldcg(I.spk_meta + 4 * o + 0);
-            s_off[i] = __ldcg(I.spk_meta + 4 * o + 1);
-            s_r0[i] = __ldcg(I.spk_meta + 4 * o + 2);
-            s_len0[i] = __ldcg(I.spk_meta + 4 * o + 3);
-            s_v[2 * i] = __ldcg(I.spk_val + 2 * o);
-            s_v[2 * i + 1] = __ldcg(I.spk_val + 2 * o + 1);
+            const uint4 m = __ldcg(reinterpret_cast<const uint4*>(I.spk_meta + 4 * o));
+            const double2 v = __ldcg(reinterpret_cast<const double2*>(I.spk_val + 2 * o));
+            s_src[i] = m.x;
+            s_off[i] = m.y;
+            s_r0[i] = m.z;
+            s_len0[i] = m.w;
+            s_v[2 * i] = v.x;
+            s_v[2 * i + 1] = v.y;
         }
         if (threadIdx.x == 0)
             s_off[nb] = b0 + nb < n ? __ldcg(I.spk_meta + 4 * (base + b0 + nb) + 1) : total;
@@ -433,79 +632,127 @@ __device__ void push_role(const InstDev& I, const Work& wk, std::int64_t step) {
     }
 }
 
-__device__ void astro_role(const InstDev& I, const Work& wk, std::int64_t step) {
-    if (threadIdx.x >= wk.count) return;
+template <bool kPdl>
+__device__ void astro_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     const std::uint32_t a = wk.first + threadIdx.x;
-    const int slot = static_cast<int>(step % I.slots);
-    unsigned long long* sp = I.ring_as.sum + static_cast<std::size_t>(slot) * I.ring_as.n_targets + a;
-    const unsigned long long g = __ldcg(sp);
-    double ca = I.Ca[a], ip3 = I.IP3[a], hh = I.h[a];
-    double ip3_in = 0.0;
-    if (g != 0) {
-        *sp = 0;
-        const double v = ring_gather<false>(I.ring_as, slot, a, g);
-        if (v != 0.0) ip3_in += v;
+    const bool active = threadIdx.x < wk.count;
+    double ca_tot = I.Ca_tot_u, ip3_0 = I.IP3_0_u, tau = I.tau_u, inv_tau = I.inv_tau_u,
+           delta = I.delta_u;
+    if (active && !I.astro_uniform) {
+        ca_tot = I.Ca_tot[a];
+        ip3_0 = I.IP3_0[a];
+        tau = I.tau[a];
+        inv_tau = I.inv_tau[a];
+        delta = I.delta[a];
     }
-    // drive_astrocytes (network.cpp:340-355)
+    if (kPdl) grid_dep_wait();
+    const std::int64_t step = S.step;
+    if (!active || step >= I.end_step) return;
+    const std::uint32_t slot = S.slot;
+    const std::size_t ts = static_cast<std::size_t>(slot) * I.ring_as.n_targets + a;
+    const std::uint32_t n = __ldcg(I.ring_as.cnt + ts);
+    double ca = I.Ca[a], ip3 = I.IP3[a], hh = I.h[a];
+    // drive_astrocytes (network.cpp:340-355) and the noise draw
+    // (astrocyte.cpp:307-329): no memory, overlapping the loads.
+    int ev = 0;
     if (I.a_rate > 0.0) {
         Draws r(I.seed ^ kSaltAstroPoisson, static_cast<std::uint64_t>(step) * kStreamStride + a);
-        const int ev = r.poisson(I.a_lambda, I.a_limit);
-        if (ev > 0) ip3_in += I.a_weight * static_cast<double>(ev);
+        ev = r.poisson(I.a_lambda, I.a_limit);
     }
-    // AstrocytePopulation::update (astrocyte.cpp:307-329)
     double noise = 0.0;
     if (I.a_std > 0.0) {
-        const std::uint64_t idx = static_cast<std::uint64_t>(step / I.a_steps_per_noise);
         const std::uint64_t nseed = I.seed ^ kSaltAstroNoise;
-        noise = I.a_indep ? I.a_std * normal_clamped(nseed, idx * kStreamStride + a)
-                          : I.a_std * normal_clamped(nseed, idx);
+        noise = I.a_std * normal_clamped_at(nseed, I.a_indep ? S.noise_a * kStreamStride + a
+                                                             : S.noise_a);
     }
-    if (I.astro_uniform) {
-        astro_rk4<false>(I.ak, I.Ca_tot_u, I.IP3_0_u, I.tau_u, I.inv_tau_u, I.delta_u, ip3_in,
-                         noise, ca, ip3, hh);
-    } else {
-        astro_rk4<false>(I.ak, I.Ca_tot[a], I.IP3_0[a], I.tau[a], I.inv_tau[a], I.delta[a],
-                         ip3_in, noise, ca, ip3, hh);
+    double ip3_in = 0.0;
+    if (n) {
+        const ShortList l = load_list(I.ring_as, ts);
+        I.ring_as.cnt[ts] = 0;
+        const double v = sum_arrivals<false>(I.ring_as, slot, a, n, l);
+        if (v != 0.0) ip3_in += v;
     }
+    if (ev > 0) ip3_in += I.a_weight * static_cast<double>(ev);
+    // AstrocytePopulation::update (astrocyte.cpp:307-329)
+    astro_rk4<false>(I.ak, ca_tot, ip3_0, tau, inv_tau, delta, ip3_in, noise, ca, ip3, hh);
     I.Ca[a] = ca;
     I.IP3[a] = ip3;
     I.h[a] = hh;
     // SIC factor of this step (astrocyte.cpp:331-339), read by the SIC sums
     // of the arrival step.
-    if (step % I.sic_interval == 0) {
+    if (S.fac_now) {
         const double y = (ca - I.SIC_th) * 1000.0;
         I.fac[static_cast<std::size_t>(slot) * I.NA + a] = y <= 1.0 ? 0.0 : I.SIC_scale * log(y);
     }
-    if (I.rec_astro_max > 0 && a < I.rec_astro_max && step >= I.rec_from &&
-        (step - I.rec_from) % I.rec_every == 0) {
-        const std::size_t row =
-            static_cast<std::size_t>(((step - I.rec_from) / I.rec_every) % I.rec_rows);
+    if (I.rec_astro_max > 0 && a < I.rec_astro_max && S.rec_now) {
+        const std::size_t row = S.rec_row;
         I.rec_Ca[row * I.rec_astro_max + a] = ca;
         I.rec_IP3[row * I.rec_astro_max + a] = ip3;
     }
 }
 
-// SIC current arriving at step+1 (valid when d_a2n >= 2: its factors were
-// written by a launch that has completed).
-__device__ void sic_role(const InstDev& I, const Work& wk, std::int64_t step) {
-    const std::uint32_t t = wk.first + threadIdx.x;
-    const std::int64_t arr = step + 1;
-    const std::int64_t se = arr - I.d_a2n;
+// Part p of the SIC sum of arrival step A = step+P-p (valid when d_a2n > P:
+// its factors were written by a launch that has completed).  Part 0 starts
+// from zero, part p > 0 continues the partial sum part p-1 left at step-1,
+// the last part writes the SIC current of A = step+1.  The list entries are
+// static and are read before the wait; after it, the partial sum and one
+// batch of factor loads.  Edges are counted by the step that adds them,
+// also for arrivals past the end of the chunk (the next chunk uses them).
+template <bool kPdl>
+__device__ void sic_role(const InstDev& I, const StepInfo& S, const Work& wk) {
+    const std::uint32_t v = wk.first + threadIdx.x;  // part * sic_npad + target
+    const std::uint32_t p = v / I.sic_npad, t = v - p * I.sic_npad;
+    const std::uint32_t P = static_cast<std::uint32_t>(I.sic_parts);
+    const bool on = threadIdx.x < wk.count && t < I.N && ((S.sic_due >> p) & 1u);
+    std::uint32_t o0 = 0, len = 0, e[kSicBatch];
+    if (on) {
+        sic_prefetch(I, v, o0, len, e);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kSicBatch; ++k) e[k] = 0u;
+    }
+    if (kPdl) grid_dep_wait();
+    if (S.step >= I.end_step) return;
     unsigned long long edges = 0;
-    // Computed even when step+1 lies past this chunk: the next chunk reads it.
-    if (threadIdx.x < wk.count && se >= 0 && se % I.sic_interval == 0) {
-        I.sic_val[static_cast<std::size_t>(arr & 1) * I.N + t] =
-            sic_sum(I, t, static_cast<int>(se % I.slots), edges);
+    if (on) {
+        const std::size_t part_n = static_cast<std::size_t>(P - 1) * I.sic_npad;
+        const double acc0 =
+            p == 0 ? 0.0
+                   : __ldcg(I.sic_part + static_cast<std::size_t>((S.step + 1) & 1) * part_n +
+                            static_cast<std::size_t>(p - 1) * I.sic_npad + t);
+        const double acc = sic_sum(I, o0, len, e, S.sic_slot[p], acc0, edges);
+        if (p + 1 == P) {
+            I.sic_val[static_cast<std::size_t>((S.step + 1) & 1) * I.N + t] = acc;
+        } else {
+            I.sic_part[static_cast<std::size_t>(S.step & 1) * part_n +
+                       static_cast<std::size_t>(p) * I.sic_npad + t] = acc;
+        }
     }
     // one atomic per warp
     for (int o = 16; o > 0; o >>= 1) edges += __shfl_down_sync(0xFFFFFFFFu, edges, o);
     if ((threadIdx.x & 31) == 0 && edges) atomicAdd(I.counters + 1, edges);
 }
 
+template <bool kPdl>
+__device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, const Work& wk) {
+    if (wk.role == kRoleNeuron) {
+        neuron_role<kPdl>(I, S, wk);
+    } else if (wk.role == kRoleAstro) {
+        astro_role<kPdl>(I, S, wk);
+    } else if (wk.role == kRolePush) {
+        push_role<kPdl>(I, S, wk);
+    } else {
+        sic_role<kPdl>(I, S, wk);
+    }
+}
+
 __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restrict__ insts,
                                                          const Work* __restrict__ work, int k) {
-    // Stage this block's instance descriptor in shared memory.
+    // Stage this block's instance descriptor and step arithmetic in shared
+    // memory.  Both depend only on data written before the chunk started, so
+    // this overlaps the tail of the previous step's grid.
     __shared__ __align__(16) unsigned char s_raw[sizeof(InstDev)];
+    __shared__ StepInfo s_info;
     const Work wk = work[blockIdx.x];
     {
         const auto* src = reinterpret_cast<const std::uint32_t*>(insts + wk.inst);
@@ -514,23 +761,13 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restri
     }
     __syncthreads();
     const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
+    if (threadIdx.x == 0) make_step_info(I, I.step0 + k, s_info);
+    __syncthreads();
     // Programmatic dependent launch: let the next step's grid be scheduled
-    // now, and wait here until the previous step's grid has completed and
-    // its memory is visible.  The descriptor and work table read above were
-    // written before the chunk started.
+    // now.  Each role waits (griddepcontrol.wait) for this launch's
+    // predecessor to complete before touching state it writes.
     asm volatile("griddepcontrol.launch_dependents;");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    const std::int64_t step = I.step0 + k;
-    if (step >= I.end_step) return;
-    if (wk.role == kRoleNeuron) {
-        neuron_role(I, wk, step);
-    } else if (wk.role == kRoleAstro) {
-        astro_role(I, wk, step);
-    } else if (wk.role == kRolePush) {
-        push_role(I, wk, step);
-    } else {
-        sic_role(I, wk, step);
-    }
+    run_role<true>(I, s_info, wk);
 }
 
 // Grid-wide barrier of the persistent chunk kernel (all blocks co-resident
@@ -585,6 +822,7 @@ __global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restr
                                                           int n_work, int steps,
                                                           GridBarrier* gb) {
     __shared__ __align__(16) unsigned char s_raw[sizeof(InstDev)];
+    __shared__ StepInfo s_info;
     __shared__ unsigned s_inst;
     if (threadIdx.x == 0) s_inst = 0xFFFFFFFFu;
     const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
@@ -599,20 +837,10 @@ __global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restr
                     dst[i] = src[i];
                 __syncthreads();
                 if (threadIdx.x == 0) s_inst = wk.inst;
-                __syncthreads();
             }
-            const std::int64_t step = I.step0 + k;
-            if (step < I.end_step) {
-                if (wk.role == kRoleNeuron) {
-                    neuron_role(I, wk, step);
-                } else if (wk.role == kRoleAstro) {
-                    astro_role(I, wk, step);
-                } else if (wk.role == kRolePush) {
-                    push_role(I, wk, step);
-                } else {
-                    sic_role(I, wk, step);
-                }
-            }
+            if (threadIdx.x == 0) make_step_info(I, I.step0 + k, s_info);
+            __syncthreads();
+            if (s_info.step < I.end_step) run_role<false>(I, s_info, wk);
         }
         if (k + 1 < steps && !grid_sync(gb, gridDim.x)) return;
     }
