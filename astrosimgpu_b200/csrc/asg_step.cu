@@ -48,35 +48,64 @@ struct StepInfo {
     std::int32_t sic_now, fac_now, rec_now;
 };
 
+// Computed by warp 0 of the block: each lane forms one quotient and
+// remainder (of a step offset by a period), so the whole set costs the
+// latency of one 64-bit division instead of some twenty in a row.
 __device__ void make_step_info(const InstDev& I, std::int64_t step, StepInfo& S) {
-    const std::int64_t slots = I.slots;
-    S.step = step;
-    S.slot = static_cast<std::uint32_t>(step % slots);
-    const std::int64_t se = step - I.d_a2n;
-    S.sic_now = se >= 0 && se % I.sic_interval == 0;
-    S.fslot = se >= 0 ? static_cast<std::uint32_t>(se % slots) : 0u;
-    S.sic_due = 0;
-    for (int p = 0; p < I.sic_parts; ++p) {
-        const std::int64_t sp = step + I.sic_parts - p - I.d_a2n;
-        const bool due = sp >= 0 && sp % I.sic_interval == 0;
-        S.sic_due |= due ? (1u << p) : 0u;
-        S.sic_slot[p] = due ? static_cast<std::uint32_t>(sp % slots) : 0u;
+    __shared__ long long s_q[32], s_r[32];
+    const int lane = static_cast<int>(threadIdx.x);
+    const int P = I.sic_parts;
+    std::int64_t n = step, d = I.slots;  // lane 0: ring slot
+    if (lane == 1) { n = step - I.d_a2n; d = I.sic_interval; }
+    if (lane == 2) { n = step - I.d_a2n; }
+    if (lane == 3) { n = step - 1 + I.d_e; }
+    if (lane == 4) { n = step - 1 + I.d_i; }
+    if (lane == 5) { n = step + I.d_e; }
+    if (lane == 6) { n = step + I.d_i; }
+    if (lane == 7) { d = 3; }
+    if (lane == 8) { d = I.sic_interval; }
+    if (lane == 9) { n = step - I.rec_from; d = I.rec_every; }
+    if (lane == 10) { d = I.pe.steps_per_noise; }
+    if (lane == 11) { d = I.pi.steps_per_noise; }
+    if (lane == 12) { d = I.a_steps_per_noise; }
+    if (lane >= 13 && lane < 13 + P) { n = step + P - (lane - 13) - I.d_a2n; d = I.sic_interval; }
+    if (lane >= 13 + P && lane < 13 + 2 * P) { n = step + P - (lane - 13 - P) - I.d_a2n; }
+    std::int64_t q = -1, r = -1;  // -1: negative numerator (not yet due)
+    if (n >= 0) {
+        const auto un = static_cast<unsigned long long>(n), ud = static_cast<unsigned long long>(d);
+        q = static_cast<std::int64_t>(un / ud);
+        r = static_cast<std::int64_t>(un - static_cast<unsigned long long>(q) * ud);
     }
-    S.push_e = static_cast<std::uint32_t>((step - 1 + I.d_e) % slots);
-    S.push_i = static_cast<std::uint32_t>((step - 1 + I.d_i) % slots);
-    S.now_e = static_cast<std::uint32_t>((step + I.d_e) % slots);
-    S.now_i = static_cast<std::uint32_t>((step + I.d_i) % slots);
-    S.ls = static_cast<std::uint32_t>(step % 3);
-    S.ls_prev = static_cast<std::uint32_t>((step + 2) % 3);
-    S.ls_next = static_cast<std::uint32_t>((step + 1) % 3);
-    S.fac_now = step % I.sic_interval == 0;
-    S.rec_now = step >= I.rec_from && (step - I.rec_from) % I.rec_every == 0;
-    S.rec_row = S.rec_now ? static_cast<std::uint32_t>(((step - I.rec_from) / I.rec_every) %
-                                                       static_cast<std::int64_t>(I.rec_rows))
-                          : 0u;
-    S.noise_e = static_cast<std::uint64_t>(step / I.pe.steps_per_noise);
-    S.noise_i = static_cast<std::uint64_t>(step / I.pi.steps_per_noise);
-    S.noise_a = static_cast<std::uint64_t>(step / I.a_steps_per_noise);
+    s_q[lane] = q;
+    s_r[lane] = r;
+    __syncwarp();
+    if (lane == 0) {
+        S.step = step;
+        S.slot = static_cast<std::uint32_t>(s_r[0]);
+        S.sic_now = s_r[1] == 0;
+        S.fslot = s_r[2] >= 0 ? static_cast<std::uint32_t>(s_r[2]) : 0u;
+        S.sic_due = 0;
+        for (int p = 0; p < P; ++p) {
+            const bool due = s_r[13 + p] == 0;
+            S.sic_due |= due ? (1u << p) : 0u;
+            S.sic_slot[p] = due ? static_cast<std::uint32_t>(s_r[13 + P + p]) : 0u;
+        }
+        S.push_e = static_cast<std::uint32_t>(s_r[3]);
+        S.push_i = static_cast<std::uint32_t>(s_r[4]);
+        S.now_e = static_cast<std::uint32_t>(s_r[5]);
+        S.now_i = static_cast<std::uint32_t>(s_r[6]);
+        S.ls = static_cast<std::uint32_t>(s_r[7]);
+        S.ls_prev = (S.ls + 2) % 3;
+        S.ls_next = (S.ls + 1) % 3;
+        S.fac_now = s_r[8] == 0;
+        S.rec_now = s_r[9] == 0;
+        S.rec_row = S.rec_now ? static_cast<std::uint32_t>(
+                                    static_cast<unsigned long long>(s_q[9]) % I.rec_rows)
+                              : 0u;
+        S.noise_e = static_cast<std::uint64_t>(s_q[10]);
+        S.noise_i = static_cast<std::uint64_t>(s_q[11]);
+        S.noise_a = static_cast<std::uint64_t>(s_q[12]);
+    }
 }
 
 // Routes one arrival the way NeuronPopulation::add_synaptic_input does
@@ -761,7 +790,7 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restri
     }
     __syncthreads();
     const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
-    if (threadIdx.x == 0) make_step_info(I, I.step0 + k, s_info);
+    if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
     __syncthreads();
     // Programmatic dependent launch: let the next step's grid be scheduled
     // now.  Each role waits (griddepcontrol.wait) for this launch's
@@ -838,7 +867,7 @@ __global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restr
                 __syncthreads();
                 if (threadIdx.x == 0) s_inst = wk.inst;
             }
-            if (threadIdx.x == 0) make_step_info(I, I.step0 + k, s_info);
+            if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
             __syncthreads();
             if (s_info.step < I.end_step) run_role<false>(I, s_info, wk);
         }
