@@ -49,7 +49,13 @@ int DevBuf::alloc(std::size_t bytes, bool zero) {
     }
     ASG_CUDA(cudaMalloc(&p_, bytes));
     n_ = bytes;
-    if (zero) ASG_CUDA(cudaMemset(p_, 0, bytes));
+    if (zero) {
+        // The engines work on non-blocking streams, which do not wait for the
+        // legacy stream: finish the zeroing here, or a later copy on an
+        // engine stream could land first and be overwritten.
+        ASG_CUDA(cudaMemsetAsync(p_, 0, bytes, cudaStreamLegacy));
+        ASG_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
+    }
     return ASG_OK;
 }
 

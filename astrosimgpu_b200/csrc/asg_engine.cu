@@ -668,6 +668,7 @@ int Engine::rebuild() {
     // Push and SIC blocks first (longest dependent chains), then neurons, then
     // astrocytes.  A PUSH item's `first` is its index among the instance's
     // push blocks.
+    std::vector<std::uint32_t> helpers(insts.size(), 0);
     for (int role = 0; role < 4; ++role) {
         for (std::size_t s = 0; s < insts.size(); ++s) {
             const InstDev& D = insts[s]->dev;
@@ -679,18 +680,24 @@ int Engine::rebuild() {
             if (r == kRolePush) {
                 if (!D.deferred_push) continue;
                 for (int pb = 0; pb < D.push_blocks; ++pb)
-                    work.push_back(Work{static_cast<std::uint32_t>(s), r, 0,
+                    work.push_back(Work{static_cast<std::uint32_t>(s), r, kNoHelper,
                                         static_cast<std::uint32_t>(pb), 0});
                 continue;
             }
             const std::uint32_t n = r == kRoleAstro ? D.NA
                                     : r == kRoleSic ? static_cast<std::uint32_t>(D.sic_parts) * D.sic_npad
                                                     : D.N;
-            for (std::uint32_t f = 0; f < n; f += B)
-                work.push_back(Work{static_cast<std::uint32_t>(s), r, 0, f,
+            for (std::uint32_t f = 0; f < n; f += B) {
+                const std::uint16_t h = D.deferred_push && helpers[s] < kNoHelper
+                                            ? static_cast<std::uint16_t>(helpers[s]++)
+                                            : kNoHelper;
+                work.push_back(Work{static_cast<std::uint32_t>(s), r, h, f,
                                     std::min<std::uint32_t>(B, n - f)});
+            }
         }
     }
+    for (std::size_t s = 0; s < insts.size(); ++s)
+        insts[s]->dev.push_helpers = static_cast<std::int32_t>(helpers[s]);
     if (insts.size() > cap_insts || work.size() * sizeof(Work) > d_work.bytes()) {
         const std::size_t cap = std::max<std::size_t>(insts.size(), 1);
         if (cap > cap_insts) {
@@ -727,9 +734,11 @@ int Engine::rebuild() {
         cudaGraph_t g = nullptr;
         ASG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t le = cudaSuccess;
+        // The first step of a chunk follows the descriptor copy: no early
+        // (programmatic) launch for it.
         for (int k = 0; k < cfg.chunk_steps && le == cudaSuccess; ++k)
             le = launch_step(d_insts.as<InstDev>(), d_work.as<Work>(),
-                             static_cast<int>(work.size()), B, k, cfg.pdl, stream);
+                             static_cast<int>(work.size()), B, k, cfg.pdl && k > 0, stream);
         const cudaError_t ce = cudaStreamEndCapture(stream, &g);
         if (le != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
@@ -783,7 +792,8 @@ int Engine::launch_chunk(int parity, int steps) {
     } else {
         for (int k = 0; k < steps; ++k)
             ASG_CUDA(launch_step(d_insts.as<InstDev>(), d_work.as<Work>(),
-                                 static_cast<int>(work.size()), cfg.block, k, cfg.pdl, stream));
+                                 static_cast<int>(work.size()), cfg.block, k, cfg.pdl && k > 0,
+                                 stream));
     }
     const int launched = persistent_grid > 0 ? 1 : steps;
     last_kernels += launched;

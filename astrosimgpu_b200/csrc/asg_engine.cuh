@@ -64,10 +64,12 @@ enum Role : std::uint16_t { kRoleNeuron = 0, kRoleAstro = 1, kRoleSic = 2, kRole
 struct Work {
     std::uint32_t inst;
     std::uint16_t role;
-    std::uint16_t pad;
+    std::uint16_t helper;  // rank among the instance's push helpers (kNoHelper: none)
     std::uint32_t first;
     std::uint32_t count;
 };
+
+constexpr std::uint16_t kNoHelper = 0xFFFFu;
 
 // Incoming-edge structure of one arrival ring (transpose of a source CSR).
 constexpr int kListCap = 4;      // arrivals per (slot, target) held in the short list
@@ -132,6 +134,10 @@ struct InstDev {
     // spike count.  Three list slots rotate: append (s), push (s-1), reset (s+1).
     std::int32_t deferred_push;
     std::int32_t push_blocks;          // PUSH work items of this instance
+    // In a burst (many more spike edges than push threads) every other work
+    // item of the instance joins the push after its own role: push_helpers
+    // of them, ranks push_blocks.. in the flat edge space.
+    std::int32_t push_helpers;
     unsigned long long* spk_packed;    // [3]: count << 40 | edges
     std::uint32_t* spk_meta;           // [3][N][4]: source, edge offset, row0 start, row0 length
     double* spk_val;                   // [3][N][2]: exc or inh set value, n2a value

@@ -31,6 +31,18 @@ __device__ __forceinline__ void grid_dep_wait() {
     asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
+__device__ __forceinline__ Work load_work(const Work* p) {
+    static_assert(sizeof(Work) == 16, "Work is one 16-byte load");
+    const uint4 v = __ldcg(reinterpret_cast<const uint4*>(p));
+    Work w;
+    w.inst = v.x;
+    w.role = static_cast<std::uint16_t>(v.y & 0xFFFFu);
+    w.helper = static_cast<std::uint16_t>(v.y >> 16);
+    w.first = v.z;
+    w.count = v.w;
+    return w;
+}
+
 // Everything about the current step that is the same for a whole block.
 struct StepInfo {
     std::int64_t step;
@@ -597,28 +609,24 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
     }
 }
 
-// Deferred push of the spikes of step-1.  The instance's PUSH blocks stride
+// Deferred push of the spikes of step-1.  The participating blocks stride
 // over the flat edge space of that step (edge x belongs to the spike whose
 // range holds it, found by binary search in shared memory), so the work is
-// split evenly whatever the number of spikes.  One thread also clears the
-// list slot the next step appends to.
+// split evenly whatever the number of spikes.
 constexpr int kPushBatch = 256;
 
-template <bool kPdl>
-__device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
+// The deferred push of the spikes of step-1 by participant `rank` of
+// `nranks` (each a block): edge x of the flat edge space goes to thread
+// x % (nranks * blockDim.x) of the participants.
+__device__ void push_spikes(const InstDev& I, const StepInfo& S, unsigned long long packed,
+                            std::uint32_t rank, std::uint32_t nranks) {
     __shared__ std::uint32_t s_off[kPushBatch + 1], s_src[kPushBatch], s_r0[kPushBatch],
         s_len0[kPushBatch];
     __shared__ double s_v[2 * kPushBatch];
-    if (kPdl) grid_dep_wait();
-    const std::int64_t step = S.step;
-    if (step >= I.end_step) return;
-    if (wk.first == 0 && threadIdx.x == 0) I.spk_packed[S.ls_next] = 0;
-    if (step == 0) return;
-    const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev);
     const std::uint32_t n = static_cast<std::uint32_t>(packed >> 40);
     const std::uint32_t total = static_cast<std::uint32_t>(packed & 0xFFFFFFFFFFull);
-    const std::uint32_t stride = blockDim.x * I.push_blocks;
-    const std::uint32_t gtid = wk.first * blockDim.x + threadIdx.x;
+    const std::uint32_t stride = blockDim.x * nranks;
+    const std::uint32_t gtid = rank * blockDim.x + threadIdx.x;
     const std::uint32_t as_e = S.push_e, as_i = S.push_i;
     const std::size_t base = static_cast<std::size_t>(S.ls_prev) * I.N;
     for (std::uint32_t b0 = 0; b0 < n; b0 += kPushBatch) {
@@ -659,6 +667,39 @@ __device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
             }
         }
     }
+}
+
+// A burst: more than kBurstEdgesPerThread spike edges per push thread.
+constexpr std::uint32_t kBurstEdgesPerThread = 4;
+
+__device__ __forceinline__ bool push_burst(const InstDev& I, unsigned long long packed) {
+    return (packed & 0xFFFFFFFFFFull) >
+           static_cast<unsigned long long>(kBurstEdgesPerThread) * blockDim.x * I.push_blocks;
+}
+
+// Deferred push of the spikes of step-1 by the PUSH blocks (joined by every
+// other block of the instance in a burst).  One thread also clears the list
+// slot the next step appends to.
+template <bool kPdl>
+__device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
+    if (kPdl) grid_dep_wait();
+    const std::int64_t step = S.step;
+    if (step >= I.end_step) return;
+    if (wk.first == 0 && threadIdx.x == 0) I.spk_packed[S.ls_next] = 0;
+    if (step == 0) return;
+    const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev);
+    const std::uint32_t nranks = static_cast<std::uint32_t>(I.push_blocks) +
+                                 (push_burst(I, packed) ? I.push_helpers : 0u);
+    push_spikes(I, S, packed, wk.first, nranks);
+}
+
+// A non-push block's share of a burst push, after its own role.
+__device__ __noinline__ void help_push(const InstDev& I, const StepInfo& S, const Work& wk) {
+    if (!I.deferred_push || wk.helper == kNoHelper || S.step == 0 || S.step >= I.end_step) return;
+    const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev);
+    if (!push_burst(I, packed)) return;
+    push_spikes(I, S, packed, static_cast<std::uint32_t>(I.push_blocks) + wk.helper,
+                static_cast<std::uint32_t>(I.push_blocks + I.push_helpers));
 }
 
 template <bool kPdl>
@@ -764,15 +805,18 @@ __device__ void sic_role(const InstDev& I, const StepInfo& S, const Work& wk) {
 
 template <bool kPdl>
 __device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, const Work& wk) {
+    if (wk.role == kRolePush) {
+        push_role<kPdl>(I, S, wk);
+        return;
+    }
     if (wk.role == kRoleNeuron) {
         neuron_role<kPdl>(I, S, wk);
     } else if (wk.role == kRoleAstro) {
         astro_role<kPdl>(I, S, wk);
-    } else if (wk.role == kRolePush) {
-        push_role<kPdl>(I, S, wk);
     } else {
         sic_role<kPdl>(I, S, wk);
     }
+    help_push(I, S, wk);
 }
 
 __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restrict__ insts,
@@ -782,11 +826,14 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restri
     // this overlaps the tail of the previous step's grid.
     __shared__ __align__(16) unsigned char s_raw[sizeof(InstDev)];
     __shared__ StepInfo s_info;
-    const Work wk = work[blockIdx.x];
+    // Through L2 (never a cached line of an earlier chunk or engine): the
+    // descriptors are rewritten by a host copy before every chunk.
+    const Work wk = load_work(work + blockIdx.x);
     {
         const auto* src = reinterpret_cast<const std::uint32_t*>(insts + wk.inst);
         auto* dst = reinterpret_cast<std::uint32_t*>(s_raw);
-        for (unsigned i = threadIdx.x; i < sizeof(InstDev) / 4; i += blockDim.x) dst[i] = src[i];
+        for (unsigned i = threadIdx.x; i < sizeof(InstDev) / 4; i += blockDim.x)
+            dst[i] = __ldcg(src + i);
     }
     __syncthreads();
     const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
@@ -857,13 +904,13 @@ __global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restr
     const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
     for (int k = 0; k < steps; ++k) {
         for (int wi = blockIdx.x; wi < n_work; wi += gridDim.x) {
-            const Work wk = work[wi];
+            const Work wk = load_work(work + wi);
             __syncthreads();
             if (s_inst != wk.inst) {
                 const auto* src = reinterpret_cast<const std::uint32_t*>(insts + wk.inst);
                 auto* dst = reinterpret_cast<std::uint32_t*>(s_raw);
                 for (unsigned i = threadIdx.x; i < sizeof(InstDev) / 4; i += blockDim.x)
-                    dst[i] = src[i];
+                    dst[i] = __ldcg(src + i);
                 __syncthreads();
                 if (threadIdx.x == 0) s_inst = wk.inst;
             }

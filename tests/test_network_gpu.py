@@ -136,6 +136,27 @@ def test_variant_parity(label, cfg):
         assert g.counters()["sic_edges"] > 0
 
 
+def test_burst_push_paths_bitwise():
+    """The initial burst of the paper-sparse network (up to ~400 spikes in a
+    step, tens of arrivals per target and slot): the deferred push with every
+    block helping, the in-block push and the persistent kernel give the same
+    bits, and the short-list overflow path is taken."""
+    m = Model(config_path("paper_sparse_dt005"), pre_time=0.0)
+    outs = []
+    for opts in (dict(), dict(push_mode=1), dict(use_graphs=2, block=256)):
+        n = Network(m, record=rec_all(), **opts)
+        n.step(800)
+        outs.append((n.fetch_spikes(), n.state(), n.counters(), opts, n.current_step,
+                     n.last_timing()))
+    sp0, st0, c0 = outs[0][:3]
+    assert c0["spikes"] > 20000, outs[0][2:]  # the burst happened
+    for sp, st, c, opts, cur, tim in outs[1:]:
+        assert np.array_equal(sp[0], sp0[0]) and np.array_equal(sp[1], sp0[1]), (
+            len(sp[0]), c, opts, cur, tim, float(np.nanmean(st["V"])))
+        for k in STATE_KEYS:
+            assert np.array_equal(st[k], st0[k]), k
+
+
 def test_sic_modes_and_block_sizes_bitwise():
     """The separate SIC role and the fused form, any block size, per-step
     graph launches, plain launches and the persistent chunk kernel give
