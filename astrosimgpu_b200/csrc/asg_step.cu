@@ -165,9 +165,13 @@ __device__ __forceinline__ double accumulate(double acc, double v, bool sub) {
 
 // More than kListCap arrivals: the first kListCap (sorted, l0 < l1 < l2 <
 // l3) are merged in bit order with the later ones, which sit in the
-// target's bitmap words (visited through the summary).  Bitmap loads go out
-// in batches -- up to 8 words, then up to 8 values -- so a burst costs a few
-// round trips, not one per arrival.  Clears the summary and the words.
+// target's bitmap words (visited through the summary).  Loads go out in
+// batches -- up to 8 words, then up to 8 values -- and every batch is issued
+// at the same point of the code by all lanes of a warp: lanes with more
+// arrivals run more passes, but no lane's loads wait behind another lane's
+// (a per-lane "flush when 8 are collected" would serialize the warp's round
+// trips lane by lane).  All arrays are indexed by unrolled constants.
+// Clears the summary and the words.
 __device__ __noinline__ double merge_overflow(const InRing& R, std::uint32_t slot,
                                               std::uint32_t t, bool sub, std::uint32_t l0,
                                               std::uint32_t l1, std::uint32_t l2,
@@ -181,34 +185,6 @@ __device__ __noinline__ double merge_overflow(const InRing& R, std::uint32_t slo
     const std::uint32_t w0 = R.wbase[t], nw = R.wbase[t + 1] - w0;
     const std::uint32_t G = (nw + 63) >> 6;  // words per summary bit
     double acc = 0.0;
-    // Adds the list entries that precede `bit`.
-    auto drain = [&](std::uint32_t bit) {
-        while (l0 < bit) {
-            acc = accumulate(acc, v0, sub);
-            l0 = l1;
-            v0 = v1;
-            l1 = l2;
-            v1 = v2;
-            l2 = l3;
-            v2 = v3;
-            l3 = kNoBit;
-        }
-    };
-    std::uint32_t idx[8];
-    int n = 0;
-    auto flush = [&]() {
-        double v[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = k < n ? __ldcg(vals + idx[k]) : 0.0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (k < n) {
-                drain(idx[k]);
-                acc = accumulate(acc, v[k], sub);
-            }
-        }
-        n = 0;
-    };
     std::uint32_t q[8], wv[8];
     std::uint32_t cur = 0, cur_end = 0;  // words [cur, cur_end) of the open group
     bool open = false;
@@ -234,19 +210,58 @@ __device__ __noinline__ double merge_overflow(const InRing& R, std::uint32_t slo
         for (int k = 0; k < 8; ++k) wv[k] = k < nq ? __ldcg(bits + q[k]) : 0u;
 #pragma unroll
         for (int k = 0; k < 8; ++k)
-            if (k < nq && wv[k] != 0) bits[q[k]] = 0;
-        for (int k = 0; k < nq; ++k) {
-            std::uint32_t word = wv[k];
-            while (word != 0) {
-                const int b = __ffs(word) - 1;
-                word &= word - 1;
-                idx[n++] = q[k] * 32 + b;
-                if (n == 8) flush();
+            if (wv[k] != 0) bits[q[k]] = 0;
+        // Passes of up to 8 set bits, in ascending order over the words.
+        for (;;) {
+            std::uint32_t any = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) any |= wv[k];
+            if (any == 0) break;
+            std::uint32_t idx[8];
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                std::uint32_t w = 0, base = 0;
+                bool found = false;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const bool take = !found && wv[k] != 0;
+                    w = take ? wv[k] : w;
+                    base = take ? q[k] * 32 : base;
+                    if (take) wv[k] &= wv[k] - 1;
+                    found = found || take;
+                }
+                idx[s] = found ? base + static_cast<std::uint32_t>(__ffs(w) - 1) : kNoBit;
+            }
+            double v[8];
+#pragma unroll
+            for (int s = 0; s < 8; ++s) v[s] = idx[s] != kNoBit ? __ldcg(vals + idx[s]) : 0.0;
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                if (idx[s] == kNoBit) break;
+                while (l0 < idx[s]) {  // list entries that precede this bit
+                    acc = accumulate(acc, v0, sub);
+                    l0 = l1;
+                    v0 = v1;
+                    l1 = l2;
+                    v1 = v2;
+                    l2 = l3;
+                    v2 = v3;
+                    l3 = kNoBit;
+                }
+                acc = accumulate(acc, v[s], sub);
             }
         }
     }
-    flush();
-    drain(kNoBit);
+    while (l0 != kNoBit) {
+        acc = accumulate(acc, v0, sub);
+        l0 = l1;
+        v0 = v1;
+        l1 = l2;
+        v1 = v2;
+        l2 = l3;
+        v2 = v3;
+        l3 = kNoBit;
+    }
     return acc;
 }
 
