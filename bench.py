@@ -258,29 +258,67 @@ def bench_astro_scaling(args, rank, world, pg):
     return out, (w, Ca, IP3, h)
 
 
-def bench_network(name="paper_sparse_dt005", warm=400, steps=2000, autotune=True, **opts):
-    """Plain one-network path on a shipped config: device time per step."""
+def network_bytes(n, na, astro_uniform, spike_edges, sic_edges, steps, sic_steps):
+    """Algorithmic HBM bytes of `steps` network steps: 144 B per neuron-step,
+    56 B (uniform astrocyte parameters) or 88 B per astrocyte-step, 68 B per
+    delivered spike edge, 4 B per active SIC edge plus 8 B per astrocyte
+    factor and 8 B per neuron SIC value on each SIC step."""
+    return (144 * n + (56 if astro_uniform else 88) * na) * steps + 68 * spike_edges + \
+        4 * sic_edges + (8 * na + 8 * n) * sic_steps
+
+
+def bench_network(name="paper_sparse_dt005", calls=20, steady_calls=5, **opts):
+    """Plain one-network path: the whole simulated time of a shipped config
+    (paper_sparse_dt005: 20,000 steps = 1 s), device time per call of 1,000
+    steps, with the algorithmic-byte roofline over the whole run and over
+    its last `steady_calls` calls (the SIC-active steady state)."""
     from astrosimgpu_b200 import _lib
     from astrosimgpu_b200.network import Model, Network, config_path
+    hbm, src = load_peaks()
     t0 = time.perf_counter()
     m = Model(config_path(name), pre_time=0.0)
     build_s = time.perf_counter() - t0
+    opts.setdefault("chunk_steps", 64)
     net = Network(m, record=_lib.RecordOpts(0, 10, 1, 0, 0), **opts)
-    net.step(warm)
-    tuned = net.autotune(200) if autotune else None
-    c0 = net.counters()
-    net.step(steps)
-    ms, kernels = net.last_timing()
-    c1 = net.counters()
-    n = net.n
-    events = (c1["spike_edges"] - c0["spike_edges"]) + (c1["sic_edges"] - c0["sic_edges"])
-    us = ms * 1e3 / steps
-    return {"config": name, "neurons": n, "astrocytes": net.na, "dt_ms": m.dt,
-            "us_per_step": us, "neuron_updates_per_s": n / (us * 1e-6),
-            "synaptic_events_per_s": events / (ms * 1e-3),
-            "sim_s_per_wall_s": (m.dt * 1e-3) / (us * 1e-6), "kernels": kernels,
-            "spikes": c1["spikes"] - c0["spikes"], "build_s": build_s, "steps": steps,
-            "warm_steps": warm, "autotuned": tuned}
+    per = max(1, m.sim_steps // calls)
+    uniform = not json.load(open(config_path(name))).get("randomize_astro", {}).get("enabled", False)
+    rows = []
+    prev = net.counters()
+    kernels = 0
+    wall0 = time.perf_counter()
+    for _ in range(calls):
+        net.step(per)
+        ms, k = net.last_timing()
+        c = net.counters()
+        rows.append((ms, c["spike_edges"] - prev["spike_edges"], c["sic_edges"] - prev["sic_edges"],
+                     c["spikes"] - prev["spikes"]))
+        kernels += k
+        prev = c
+    wall_s = time.perf_counter() - wall0
+    n, na = net.n, net.na
+
+    def summary(sel):
+        ms = sum(r[0] for r in sel)
+        steps = per * len(sel)
+        se, sic = sum(r[1] for r in sel), sum(r[2] for r in sel)
+        sic_steps = steps if sic > 0 else 0
+        gb = network_bytes(n, na, uniform, se, sic, steps, sic_steps) / (ms * 1e-3) / 1e9
+        us = ms * 1e3 / steps
+        return {"steps": steps, "device_ms": ms, "us_per_step": us,
+                "sim_s_per_wall_s": (m.dt * 1e-3) / (us * 1e-6),
+                "neuron_updates_per_s": n / (us * 1e-6),
+                "synaptic_events_per_s": (se + sic) / (ms * 1e-3),
+                "roofline": {"bound": "hbm", "achieved": gb, "peak": hbm, "unit": "GB/s",
+                             "frac": gb / hbm, "peak_source": src}}
+    full = summary(rows)
+    out = {"config": name, "neurons": n, "astrocytes": na, "dt_ms": m.dt, "build_s": build_s,
+           "kernels": kernels, "spikes": sum(r[3] for r in rows),
+           "wall_s_including_host": wall_s,
+           "per_1000_steps_us_per_step": [round(r[0] * 1e3 / per, 2) for r in rows],
+           "engine_opts": opts}
+    out.update(full)
+    out["steady_state_last_%d_steps" % (per * steady_calls)] = summary(rows[-steady_calls:])
+    return out
 
 
 def bench_batched(sim_ms=500.0, n_inst=64, autotune=True):
@@ -450,9 +488,9 @@ def main():
                     help="skip the reference CUDA kernel and sub-benchmarks")
     ap.add_argument("--skip", default="", help="comma list of sub-benchmarks to skip: "
                     "network_c2,batched_c3,serving_c4")
-    ap.add_argument("--engine-mode", type=int, default=0,
-                    help="network engine launches (--only network_c2): 0 autotune, 1 graphs "
-                         "of per-step kernels, 2 persistent chunk kernel")
+    ap.add_argument("--engine-mode", type=int, default=1,
+                    help="network engine launches (--only network_c2): 1 graphs of per-step "
+                         "kernels, 2 persistent chunk kernel")
     ap.add_argument("--only", default="", choices=["", "astro", "network_c2", "batched_c3",
                                                    "serving_c4"],
                     help="run one part alone and print its JSON (profiling)")
@@ -470,9 +508,7 @@ def main():
     import torch
     torch.cuda.set_device(local)
     if args.only and args.only != "astro":
-        fn = {"network_c2": lambda: bench_network(warm=args.warmup, steps=args.steps,
-                                                  autotune=args.engine_mode == 0,
-                                                  use_graphs=max(args.engine_mode, 1)),
+        fn = {"network_c2": lambda: bench_network(use_graphs=max(args.engine_mode, 1)),
               "batched_c3": bench_batched, "serving_c4": bench_serving}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
         return 0
