@@ -117,7 +117,7 @@ struct SicHost {
     std::uint32_t max_edges = 0;  // largest number of SIC edges of one target
 };
 
-constexpr std::uint32_t kSicEdgesPerPart = 256;
+constexpr std::uint32_t kSicEdgesPerPart = 160;
 constexpr std::uint32_t kPushCells = 256;
 
 // Longest SIC edge list of one target (sets the number of parts).
