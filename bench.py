@@ -43,6 +43,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "neuron-updates/s & HBM GB/s vs roofline; batched/served vs plain; p50/p99 lat"
 BYTES_PER_CELL_STEP = 48  # Ca, IP3, h: read + write, FP64
+# dram__bytes_read.sum + dram__bytes_write.sum of one astro_step_kernel launch,
+# from an ncu --set full capture of this workload (mean of two launches).
+NCU_TRAFFIC_PER_LAUNCH = {10_000_000: 420_363_392}
 
 
 def load_peaks():
@@ -248,7 +251,9 @@ def bench_astro_scaling(args, rank, world, pg):
                 "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                 "steps": e2e_steps, "path": "asg_astro_push_input+update+pull_calcium"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": NCU_TRAFFIC_PER_LAUNCH.get(n),
+                     "traffic_unit": "bytes per launch (ncu dram read + write)",
                      "peak_source": peak_kind,
                      "bytes_per_launch": BYTES_PER_CELL_STEP * n,
                      "kernel": "astro_step_kernel<uniform,bernoulli>"},
