@@ -136,6 +136,24 @@ def test_variant_parity(label, cfg):
         assert g.counters()["sic_edges"] > 0
 
 
+def test_sic_parts_parity():
+    """SIC sums cut into parts computed on consecutive steps: a network whose
+    targets take ~350 SIC edges (three parts of ~120) with every astrocyte
+    above the SIC threshold from the start, against the oracle."""
+    cfg = json.load(open(config_path("paper_sparse_dt005")))
+    cfg["N"].update({"N_E": 2000, "N_I": 500, "N_A": 2500})
+    cfg["connectivity"]["p_primary"] = 0.35
+    cfg["astrocyte"]["Ca_init"] = 0.35
+    cfg["astrocyte"]["IP3"] = 0.6
+    text = json.dumps(cfg)
+    rs, tg = Model(text=text, pre_time=0.0).table(3)
+    assert np.bincount(tg).max() > 320  # three parts of at most 160 edges
+    g, r, gsp, rsp = run_pair(text=text, steps=400, chunks=2)
+    assert_same_spikes(gsp, rsp)
+    assert_state_close(g, r)
+    assert g.counters()["sic_edges"] > 1_000_000
+
+
 def test_burst_push_paths_bitwise():
     """The initial burst of the paper-sparse network (up to ~400 spikes in a
     step, tens of arrivals per target and slot): the deferred push with every
