@@ -536,7 +536,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     ring_segs(D.ring_in, rin, N);
     ring_segs(D.ring_as, ras, NA);
 
-    add_seg(D.spk_packed, 4 * 8, nullptr);
+    add_seg(D.spk_packed, 3 * kHeaderStride * 8, nullptr);
     add_seg(D.spk_meta, 3 * std::max<std::size_t>(N, 1) * 16, nullptr);
     add_seg(D.spk_val, 3 * std::max<std::size_t>(N, 1) * 16, nullptr);
     add_seg(D.sic_soff, sic.soff.size() * 4, sic.soff.data());

@@ -74,6 +74,7 @@ constexpr std::uint16_t kNoHelper = 0xFFFFu;
 // Incoming-edge structure of one arrival ring (transpose of a source CSR).
 constexpr int kListCap = 4;      // arrivals per (slot, target) held in the short list
 constexpr int kMaxSicParts = 8;  // most parts a target's SIC chain is cut into
+constexpr int kHeaderStride = 16;  // u64 words between spike-list headers (128 bytes)
 
 struct InRing {
     const std::uint32_t* wbase;   // [n_targets+1] first bitmap word of each target
@@ -138,7 +139,10 @@ struct InstDev {
     // item of the instance joins the push after its own role: push_helpers
     // of them, ranks push_blocks.. in the flat edge space.
     std::int32_t push_helpers;
-    unsigned long long* spk_packed;    // [3]: count << 40 | edges
+    // [3][kHeaderStride]: count << 40 | edges, one 128-byte line per slot --
+    // the slot being appended to (atomics) and the slot being read by every
+    // block must not share an L2 sector, or the reads queue behind the atomics.
+    unsigned long long* spk_packed;
     std::uint32_t* spk_meta;           // [3][N][4]: source, edge offset, row0 start, row0 length
     double* spk_val;                   // [3][N][2]: exc or inh set value, n2a value
     // SIC: sliced ELL over virtual targets v = part * sic_npad + target,

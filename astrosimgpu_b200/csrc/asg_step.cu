@@ -575,7 +575,7 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
             const double v1 = exc ? (I.stp_on ? I.w_n2a * x * u : I.w_n2a) : 0.0;
             if (I.deferred_push) {
                 const unsigned long long old = atomicAdd(
-                    I.spk_packed + S.ls,
+                    I.spk_packed + S.ls * kHeaderStride,
                     (1ull << 40) | static_cast<unsigned long long>(len0 + len1));
                 const std::size_t o = static_cast<std::size_t>(S.ls) * I.N + (old >> 40);
                 *reinterpret_cast<uint4*>(I.spk_meta + 4 * o) =
@@ -700,9 +700,9 @@ __device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     if (kPdl) grid_dep_wait();
     const std::int64_t step = S.step;
     if (step >= I.end_step) return;
-    if (wk.first == 0 && threadIdx.x == 0) I.spk_packed[S.ls_next] = 0;
+    if (wk.first == 0 && threadIdx.x == 0) I.spk_packed[S.ls_next * kHeaderStride] = 0;
     if (step == 0) return;
-    const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev);
+    const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev * kHeaderStride);
     const std::uint32_t nranks = static_cast<std::uint32_t>(I.push_blocks) +
                                  (push_burst(I, packed) ? I.push_helpers : 0u);
     push_spikes(I, S, packed, wk.first, nranks);
@@ -711,7 +711,7 @@ __device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
 // A non-push block's share of a burst push, after its own role.
 __device__ __noinline__ void help_push(const InstDev& I, const StepInfo& S, const Work& wk) {
     if (!I.deferred_push || wk.helper == kNoHelper || S.step == 0 || S.step >= I.end_step) return;
-    const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev);
+    const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev * kHeaderStride);
     if (!push_burst(I, packed)) return;
     push_spikes(I, S, packed, static_cast<std::uint32_t>(I.push_blocks) + wk.helper,
                 static_cast<std::uint32_t>(I.push_blocks + I.push_helpers));
