@@ -273,7 +273,14 @@ Engine::~Engine() {
     }
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_end) cudaEventDestroy(ev_end);
+    if (ev_side_fork) cudaEventDestroy(ev_side_fork);
+    if (ev_side_join) cudaEventDestroy(ev_side_join);
+    for (int q = 0; q < kSideEvents; ++q) {
+        if (ev_side_pre[q]) cudaEventDestroy(ev_side_pre[q]);
+        if (ev_side_done[q]) cudaEventDestroy(ev_side_done[q]);
+    }
     insts.clear();
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -295,6 +302,13 @@ int Engine::init() {
         cfg.mem_budget = static_cast<std::uint64_t>(0.9 * static_cast<double>(fr));
     }
     ASG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    ASG_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    ASG_CUDA(cudaEventCreateWithFlags(&ev_side_fork, cudaEventDisableTiming));
+    ASG_CUDA(cudaEventCreateWithFlags(&ev_side_join, cudaEventDisableTiming));
+    for (int q = 0; q < kSideEvents; ++q) {
+        ASG_CUDA(cudaEventCreateWithFlags(&ev_side_pre[q], cudaEventDisableTiming));
+        ASG_CUDA(cudaEventCreateWithFlags(&ev_side_done[q], cudaEventDisableTiming));
+    }
     ASG_CUDA(cudaEventCreate(&ev_start));
     ASG_CUDA(cudaEventCreate(&ev_end));
     for (int p = 0; p < 2; ++p) {
@@ -331,6 +345,7 @@ int Engine::footprint(const asg_network_desc& d, int chunk_steps, std::uint64_t*
     b += slots * (2 * N + NA) * (4 + kListCap * 12);                // counters, short lists
     b += Es * 4 + N * 8 + slots * NA * 8 + 2 * N * 8;  // SIC (upper bound), factors, values
     b += (N + 32) * (kMaxSicParts * 8 + 2 * kMaxSicParts * 8);  // part cuts, partial sums
+    b += N * 8 * kSicRing;                                        // SIC value ring
     b += 256 * 64;                                     // alignment slack
     (void)chunk_steps;
     *bytes = b;
@@ -451,7 +466,14 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     // of step A - d_a2n, written by an earlier launch).
     D.sic_npad = (N + 31) / 32 * 32;
     D.sic_parts = 1;
-    if (!D.fused_sic) {
+    // Side-stream SIC batches need a delay that leaves a few steps between
+    // a batch and its first reader (lead >= 4); sic_mode 2 keeps the
+    // in-kernel parts.
+    D.sic_side = (!D.fused_sic && cfg.sic_mode != 2 && NA > 0 &&
+                  D.d_a2n >= kSicBatchSteps + 4) ? 1 : 0;
+    D.sic_lead = D.sic_side ? std::min(D.d_a2n - kSicBatchSteps, kSicRing - kSicBatchSteps - 8) : 0;
+    D.sic_ring = D.sic_side ? kSicRing : 2;
+    if (!D.fused_sic && !D.sic_side) {
         const std::uint32_t mx = sic_max_edges(NA, rs_of(d.astro_neuron), d.astro_neuron.target, N);
         const int want = static_cast<int>((mx + kSicEdgesPerPart - 1) / kSicEdgesPerPart);
         D.sic_parts = std::max(1, std::min({want, kMaxSicParts, D.d_a2n - 1}));
@@ -544,7 +566,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     add_seg(D.fac, S * std::max<std::size_t>(a8, 8), nullptr);
     add_seg(D.sic_part,
             2 * static_cast<std::size_t>(std::max(D.sic_parts - 1, 1)) * D.sic_npad * 8, nullptr);
-    add_seg(D.sic_val, 2 * std::max<std::size_t>(n8, 8), nullptr);
+    add_seg(D.sic_val, static_cast<std::size_t>(D.sic_ring) * std::max<std::size_t>(n8, 8), nullptr);
 
     std::size_t total = 0;
     for (const Seg& s : segs) total += align256(std::max<std::size_t>(s.bytes, 1));
@@ -676,7 +698,7 @@ int Engine::rebuild() {
                                     : role == 1 ? kRoleSic
                                     : role == 2 ? kRoleNeuron
                                                 : kRoleAstro;
-            if (r == kRoleSic && D.fused_sic) continue;
+            if (r == kRoleSic && (D.fused_sic || (D.sic_side && cfg.use_graphs != 2))) continue;
             if (r == kRolePush) {
                 if (!D.deferred_push) continue;
                 for (int pb = 0; pb < D.push_blocks; ++pb)
@@ -698,6 +720,23 @@ int Engine::rebuild() {
     }
     for (std::size_t s = 0; s < insts.size(); ++s)
         insts[s]->dev.push_helpers = static_cast<std::int32_t>(helpers[s]);
+    // Side-stream SIC batches (graph and plain launches; the persistent
+    // kernel computes the single-part sums in its SIC role instead).
+    side_work.clear();
+    side_lead = 0;
+    side_lead_max = 0;
+    side_prime = true;
+    if (cfg.use_graphs != 2) {
+        for (std::size_t s = 0; s < insts.size(); ++s) {
+            const InstDev& D = insts[s]->dev;
+            if (!D.sic_side) continue;
+            side_lead = side_lead == 0 ? D.sic_lead : std::min(side_lead, D.sic_lead);
+            side_lead_max = std::max(side_lead_max, static_cast<int>(D.sic_lead));
+            for (std::uint32_t f = 0; f < D.N; f += B)
+                side_work.push_back(Work{static_cast<std::uint32_t>(s), kRoleSic, kNoHelper, f,
+                                         std::min<std::uint32_t>(B, D.N - f)});
+        }
+    }
     if (insts.size() > cap_insts || work.size() * sizeof(Work) > d_work.bytes()) {
         const std::size_t cap = std::max<std::size_t>(insts.size(), 1);
         if (cap > cap_insts) {
@@ -721,6 +760,11 @@ int Engine::rebuild() {
     if (!work.empty())
         ASG_CUDA(cudaMemcpyAsync(d_work.get(), work.data(), work.size() * sizeof(Work),
                                  cudaMemcpyHostToDevice, stream));
+    if (side_work.size() * sizeof(Work) > d_side_work.bytes())
+        ASG_TRY(d_side_work.alloc(side_work.size() * 2 * sizeof(Work)));
+    if (!side_work.empty())
+        ASG_CUDA(cudaMemcpyAsync(d_side_work.get(), side_work.data(),
+                                 side_work.size() * sizeof(Work), cudaMemcpyHostToDevice, stream));
     ASG_CUDA(cudaMemsetAsync(d_stats.get(), 0, cap_insts * 8 * sizeof(unsigned long long), stream));
     ASG_CUDA(cudaStreamSynchronize(stream));
     graph_steps = 0;
@@ -733,12 +777,7 @@ int Engine::rebuild() {
     if ((cfg.use_graphs == 0 || cfg.use_graphs == 1) && !work.empty()) {
         cudaGraph_t g = nullptr;
         ASG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t le = cudaSuccess;
-        // The first step of a chunk follows the descriptor copy: no early
-        // (programmatic) launch for it.
-        for (int k = 0; k < cfg.chunk_steps && le == cudaSuccess; ++k)
-            le = launch_step(d_insts.as<InstDev>(), d_work.as<Work>(),
-                             static_cast<int>(work.size()), B, k, cfg.pdl && k > 0, stream);
+        const cudaError_t le = issue_steps(cfg.chunk_steps);
         const cudaError_t ce = cudaStreamEndCapture(stream, &g);
         if (le != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
@@ -752,6 +791,64 @@ int Engine::rebuild() {
     }
     dirty = false;
     return ASG_OK;
+}
+
+// The launches of `steps` steps on the engine stream, with the side-stream
+// SIC batches: before step k (k a multiple of kSicBatchSteps) the side stream
+// waits for the steps before k and runs the batch for the arrival steps
+// step0+k+lead..; the step k+lead (the first reader, lead the smallest over
+// the instances) waits for that batch.  The side stream joins the engine
+// stream at the end, so nothing of a chunk outlives it.  The first step of a
+// chunk follows the descriptor copy: no early (programmatic) launch for it.
+cudaError_t Engine::issue_steps(int steps) {
+    const bool side_on = !side_work.empty();
+    const int G = kSicBatchSteps;
+    cudaError_t e = cudaSuccess;
+    if (side_on) {
+        e = cudaEventRecord(ev_side_fork, stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(side, ev_side_fork, 0);
+    }
+    for (int k = 0; k < steps && e == cudaSuccess; ++k) {
+        if (side_on && k % G == 0) {
+            cudaEvent_t before = ev_side_pre[(k / G) % kSideEvents];
+            cudaEvent_t done = ev_side_done[(k / G) % kSideEvents];
+            e = cudaEventRecord(before, stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(side, before, 0);
+            if (e == cudaSuccess)
+                e = launch_sic_batch(d_insts.as<InstDev>(), d_side_work.as<Work>(),
+                                     static_cast<int>(side_work.size()), cfg.block, k, side);
+            if (e == cudaSuccess) e = cudaEventRecord(done, side);
+        }
+        // (A step that waits for a batch still launches early: it reads the
+        // SIC values after griddepcontrol.wait, and the batch is a completed
+        // prerequisite by then whichever way the wait is honoured.)
+        if (side_on && k >= side_lead && (k - side_lead) % G == 0 && e == cudaSuccess)
+            e = cudaStreamWaitEvent(stream, ev_side_done[((k - side_lead) / G) % kSideEvents], 0);
+        if (e == cudaSuccess)
+            e = launch_step(d_insts.as<InstDev>(), d_work.as<Work>(), static_cast<int>(work.size()),
+                            cfg.block, k, cfg.pdl && k > 0, stream);
+    }
+    if (side_on && e == cudaSuccess) {
+        e = cudaEventRecord(ev_side_join, side);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, ev_side_join, 0);
+    }
+    return e;
+}
+
+// SIC values of the arrival steps step0 .. step0+lead-1 of every side
+// instance, before the chunk's own batches take over (batches with k < 0;
+// arrivals before step0 are skipped in the kernel).
+cudaError_t Engine::prime_side() {
+    const int G = kSicBatchSteps;
+    cudaError_t e = cudaEventRecord(ev_side_fork, stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(side, ev_side_fork, 0);
+    const int first = -((side_lead_max + G - 1) / G) * G;
+    for (int k = first; k < 0 && e == cudaSuccess; k += G)
+        e = launch_sic_batch(d_insts.as<InstDev>(), d_side_work.as<Work>(),
+                             static_cast<int>(side_work.size()), cfg.block, k, side);
+    if (e == cudaSuccess) e = cudaEventRecord(ev_side_join, side);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, ev_side_join, 0);
+    return e;
 }
 
 int Engine::launch_chunk(int parity, int steps) {
@@ -779,6 +876,10 @@ int Engine::launch_chunk(int parity, int steps) {
     ASG_CUDA(cudaEventRecord(ev_chunk0[parity], stream));
     ASG_CUDA(cudaMemcpyAsync(d_insts.get(), hi, insts.size() * sizeof(InstDev),
                              cudaMemcpyHostToDevice, stream));
+    if (side_prime) {
+        if (!side_work.empty()) ASG_CUDA(prime_side());
+        side_prime = false;
+    }
     if (persistent_grid > 0) {
         ASG_CUDA(cudaMemsetAsync(d_barrier.get(), 0, sizeof(GridBarrier), stream));
         ASG_CUDA(launch_chunk_persistent(d_insts.as<InstDev>(), d_work.as<Work>(),
@@ -790,10 +891,7 @@ int Engine::launch_chunk(int parity, int steps) {
     } else if (graph != nullptr && steps == graph_steps) {
         ASG_CUDA(cudaGraphLaunch(graph, stream));
     } else {
-        for (int k = 0; k < steps; ++k)
-            ASG_CUDA(launch_step(d_insts.as<InstDev>(), d_work.as<Work>(),
-                                 static_cast<int>(work.size()), cfg.block, k, cfg.pdl && k > 0,
-                                 stream));
+        ASG_CUDA(issue_steps(steps));
     }
     const int launched = persistent_grid > 0 ? 1 : steps;
     last_kernels += launched;

@@ -75,6 +75,8 @@ constexpr std::uint16_t kNoHelper = 0xFFFFu;
 constexpr int kListCap = 4;      // arrivals per (slot, target) held in the short list
 constexpr int kMaxSicParts = 8;  // most parts a target's SIC chain is cut into
 constexpr int kHeaderStride = 16;  // u64 words between spike-list headers (128 bytes)
+constexpr int kSicBatchSteps = 8;  // arrival steps per side-stream SIC batch
+constexpr int kSicRing = 32;       // SIC value slots of an instance with side batches
 
 struct InRing {
     const std::uint32_t* wbase;   // [n_targets+1] first bitmap word of each target
@@ -146,14 +148,21 @@ struct InstDev {
     std::uint32_t* spk_meta;           // [3][N][4]: source, edge offset, row0 start, row0 length
     double* spk_val;                   // [3][N][2]: exc or inh set value, n2a value
     // SIC: sliced ELL over virtual targets v = part * sic_npad + target,
-    // factors per emission slot, partial sums between parts, final values
+    // factors per emission slot, partial sums between parts, final values.
+    // With sic_side the currents are computed off the step kernels, by
+    // side-stream batches: the batch launched before step s (s a multiple of
+    // kSicBatchSteps in the chunk) covers the arrival steps s+sic_lead ..
+    // s+sic_lead+kSicBatchSteps-1, one whole chain per thread (P = 1).
+    std::int32_t sic_side;
+    std::int32_t sic_lead;
+    std::int32_t sic_ring;          // slots of sic_val, a power of two
     std::int32_t sic_parts;         // P (1 when the delay is too short to split)
     std::uint32_t sic_npad;         // N rounded up to a multiple of 32
     const std::uint32_t* sic_soff;  // [P*sic_npad/32+1] entry offset of each 32-target slice
     const std::uint32_t* sic_ent;   // astro << 8 | mult
     double* fac;                    // [slots][NA]
     double* sic_part;               // [2][P-1][sic_npad] partial sums, by step parity
-    double* sic_val;                // [2][N]
+    double* sic_val;                // [sic_ring][N], slot = arrival step % sic_ring
     // outputs (host-mapped memory)
     unsigned long long* spike_log;  // (step << 32) | source
     unsigned long long* spike_log_n;
@@ -181,6 +190,11 @@ int persistent_blocks(int block);
 cudaError_t launch_chunk_persistent(const InstDev* insts, const Work* work, int n_work,
                                     int block, int grid, int steps, GridBarrier* gb,
                                     cudaStream_t stream);
+
+// One side-stream SIC batch (instances with sic_side): the arrival steps
+// step0+k+sic_lead .. +kSicBatchSteps-1 of every work item's targets.
+cudaError_t launch_sic_batch(const InstDev* insts, const Work* work, int n_work, int block, int k,
+                             cudaStream_t stream);
 
 // One step launch; with `pdl` the launch may start while the previous kernel
 // of the stream is still running (the kernel waits for it before any access

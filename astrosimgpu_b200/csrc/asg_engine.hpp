@@ -101,12 +101,18 @@ public:
     cudaStream_t stream = nullptr;
     int sms = 148;
 
+    // The next chunk first recomputes the SIC values of the arrival steps
+    // step .. step+lead-1 (after a restore: the ring may come from another
+    // launch mode).
+    void mark_side_prime() { side_prime = true; }
+
     int set_block(int block);
     int set_chunk(int chunk);
     int set_mode(int use_graphs);
 
 private:
     int rebuild();          // work table + graph after the instance set changed
+    cudaError_t issue_steps(int steps);  // step launches + side-stream SIC batches
     int launch_chunk(int parity, int steps);
     int collect(int parity);
     int finish_pending();
@@ -124,6 +130,16 @@ private:
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     bool dirty = true;
+    // side-stream SIC batches (instances with InstDev::sic_side)
+    static constexpr int kSideEvents = 8;
+    cudaStream_t side = nullptr;
+    std::vector<Work> side_work;
+    DevBuf d_side_work;
+    int side_lead = 0, side_lead_max = 0;
+    bool side_prime = true;
+    cudaError_t prime_side();
+    cudaEvent_t ev_side_fork = nullptr, ev_side_join = nullptr;
+    cudaEvent_t ev_side_pre[kSideEvents] = {}, ev_side_done[kSideEvents] = {};
     cudaEvent_t ev_start = nullptr, ev_end = nullptr;
     cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
     cudaEvent_t ev_chunk0[2] = {nullptr, nullptr};

@@ -438,7 +438,8 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
         const std::uint32_t n_in = __ldcg(I.ring_in.cnt + ts_in);
         const bool sic_due = S.sic_now != 0;
         double Isic = (sic_due && !I.fused_sic)
-                          ? __ldcg(I.sic_val + static_cast<std::size_t>(step & 1) * I.N + c)
+                          ? __ldcg(I.sic_val +
+                                   static_cast<std::size_t>(step & (I.sic_ring - 1)) * I.N + c)
                           : I.Isic[c];
         double V = I.V[c], w = I.w[c], gex = I.gex[c], gin = I.gin[c];
         double dgex = I.dgex[c], dgin = I.dgin[c];
@@ -807,7 +808,7 @@ __device__ void sic_role(const InstDev& I, const StepInfo& S, const Work& wk) {
                             static_cast<std::size_t>(p - 1) * I.sic_npad + t);
         const double acc = sic_sum(I, o0, len, e, S.sic_slot[p], acc0, edges);
         if (p + 1 == P) {
-            I.sic_val[static_cast<std::size_t>((S.step + 1) & 1) * I.N + t] = acc;
+            I.sic_val[static_cast<std::size_t>((S.step + 1) & (I.sic_ring - 1)) * I.N + t] = acc;
         } else {
             I.sic_part[static_cast<std::size_t>(S.step & 1) * part_n +
                        static_cast<std::size_t>(p) * I.sic_npad + t] = acc;
@@ -937,6 +938,77 @@ __global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restr
     }
 }
 
+// Side-stream SIC batch: thread per target, its whole list (P = 1), and the
+// sums of all kSicBatchSteps arrival steps of the batch at once: for each
+// list entry the factors of the astrocyte at the arrivals' emission steps
+// are loaded together, and the m additions of the entry advance the
+// kSicBatchSteps sums side by side -- independent chains, each the SIC
+// role's sequential sum (a zero factor adds +0.0, exact since a sum that
+// starts at +0.0 and adds nonzero values is never -0.0).  One block per
+// work item, so the batch leaves the SMs to the step kernels beside it.
+// Launched when the step before step0+k has completed (the factors it
+// needs are older still), and waited for before the first step that reads it.
+__global__ void __launch_bounds__(kMaxBlock) sic_batch_kernel(const InstDev* __restrict__ insts,
+                                                              const Work* __restrict__ work,
+                                                              int k) {
+    constexpr int G = kSicBatchSteps;
+    const Work wk = load_work(work + blockIdx.x);
+    const InstDev& I = insts[wk.inst];
+    unsigned long long edges = 0;
+    if (threadIdx.x < wk.count) {
+        const std::uint32_t t = wk.first + threadIdx.x;
+        std::uint32_t o0 = 0, len = 0, e[kSicBatch];
+        sic_prefetch(I, t, o0, len, e);
+        const double* fac[G];
+        bool due[G];
+        double acc[G];
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const std::int64_t a = I.step0 + k + I.sic_lead + j;
+            const std::int64_t se = a - I.d_a2n;
+            due[j] = a >= I.step0 && se >= 0 && se % I.sic_interval == 0;
+            fac[j] = I.fac + static_cast<std::size_t>(due[j] ? se % I.slots : 0) * I.NA;
+            acc[j] = 0.0;
+        }
+        for (std::uint32_t b0 = 0;; b0 += kSicBatch) {
+            bool done = false;
+            for (int q = 0; q < kSicBatch; ++q) {
+                const std::uint32_t m = e[q] & 0xFFu;
+                if (m == 0) {
+                    done = true;  // padding ends the list
+                    break;
+                }
+                const std::uint32_t as = e[q] >> 8;
+                double c[G];
+#pragma unroll
+                for (int j = 0; j < G; ++j) {
+                    const double f = __ldcg(fac[j] + as);
+                    c[j] = I.w_a2n * f;
+                    if (due[j] && f != 0.0) edges += m;
+                    if (f == 0.0) c[j] = 0.0;
+                }
+                for (std::uint32_t r = 0; r < m; ++r) {
+#pragma unroll
+                    for (int j = 0; j < G; ++j) acc[j] += c[j];
+                }
+            }
+            if (done || b0 + kSicBatch >= len) break;
+#pragma unroll
+            for (int q = 0; q < kSicBatch; ++q) {
+                const std::uint32_t jj = b0 + kSicBatch + q;
+                e[q] = jj < len ? __ldg(I.sic_ent + o0 + jj * 32) : 0u;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const std::int64_t a = I.step0 + k + I.sic_lead + j;
+            if (due[j]) I.sic_val[static_cast<std::size_t>(a & (I.sic_ring - 1)) * I.N + t] = acc[j];
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) edges += __shfl_down_sync(0xFFFFFFFFu, edges, o);
+    if ((threadIdx.x & 31) == 0 && edges) atomicAdd(I.counters + 1, edges);
+}
+
 // Failure-detection check of the bounded barrier: block 0 never arrives, so
 // every other block's wait must run out, set the error word and return.
 __global__ void barrier_selftest_kernel(GridBarrier* gb) {
@@ -945,6 +1017,12 @@ __global__ void barrier_selftest_kernel(GridBarrier* gb) {
 }
 
 }  // namespace
+
+cudaError_t launch_sic_batch(const InstDev* insts, const Work* work, int n_work, int block, int k,
+                             cudaStream_t stream) {
+    sic_batch_kernel<<<static_cast<unsigned>(n_work), block, 0, stream>>>(insts, work, k);
+    return cudaGetLastError();
+}
 
 cudaError_t barrier_selftest(GridBarrier* gb, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};

@@ -136,22 +136,59 @@ def test_variant_parity(label, cfg):
         assert g.counters()["sic_edges"] > 0
 
 
-def test_sic_parts_parity():
-    """SIC sums cut into parts computed on consecutive steps: a network whose
-    targets take ~350 SIC edges (three parts of ~120) with every astrocyte
-    above the SIC threshold from the start, against the oracle."""
+def sic_active_config():
+    """paper_sparse_dt005 scaled to 2,500 neurons with ~350 SIC edges per
+    target (in-degree ~700) and every astrocyte above the SIC threshold from
+    the start; the SIC delay is 20 steps."""
     cfg = json.load(open(config_path("paper_sparse_dt005")))
     cfg["N"].update({"N_E": 2000, "N_I": 500, "N_A": 2500})
     cfg["connectivity"]["p_primary"] = 0.35
     cfg["astrocyte"]["Ca_init"] = 0.35
     cfg["astrocyte"]["IP3"] = 0.6
-    text = json.dumps(cfg)
+    return json.dumps(cfg)
+
+
+def test_sic_active_parity():
+    """SIC currents computed by side-stream batches (the default at a 20-step
+    delay), against the oracle."""
+    text = sic_active_config()
     rs, tg = Model(text=text, pre_time=0.0).table(3)
-    assert np.bincount(tg).max() > 320  # three parts of at most 160 edges
+    assert np.bincount(tg).max() > 320  # the in-kernel form cuts three parts
     g, r, gsp, rsp = run_pair(text=text, steps=400, chunks=2)
     assert_same_spikes(gsp, rsp)
     assert_state_close(g, r)
     assert g.counters()["sic_edges"] > 1_000_000
+
+
+def test_sic_forms_bitwise():
+    """Side-stream batches (graph and plain launches), SIC parts pipelined in
+    the step kernel (sic_mode 2), the persistent kernel's single-part role,
+    and a persistent run resumed from a checkpoint by a side-batch network
+    (which first recomputes the SIC values of the next steps): same bits."""
+    m = Model(text=sic_active_config(), pre_time=0.0)
+    outs = []
+    for opts in (dict(), dict(use_graphs=-1), dict(sic_mode=2), dict(use_graphs=2),
+                 dict(chunk_steps=24)):
+        n = Network(m, record=rec_all(), **opts)
+        n.step(200)
+        n.step(200)
+        outs.append((n.fetch_spikes(), n.state()))
+    p = Network(m, record=rec_all(), use_graphs=2)
+    p.step(200)
+    blob = p.checkpoint()
+    q = Network(m, record=rec_all())
+    q.restore(blob)
+    q.step(200)
+    sp0, st0 = outs[0]
+    tail = sp0[0] >= 200
+    sq = q.fetch_spikes()
+    assert np.array_equal(sq[0], sp0[0][tail]) and np.array_equal(sq[1], sp0[1][tail])
+    for k in STATE_KEYS:
+        assert np.array_equal(q.state()[k], st0[k]), ("resumed", k)
+    for (sp, st) in outs[1:]:
+        assert np.array_equal(sp[0], sp0[0]) and np.array_equal(sp[1], sp0[1])
+        for k in STATE_KEYS:
+            assert np.array_equal(st[k], st0[k]), k
 
 
 def test_burst_push_paths_bitwise():
