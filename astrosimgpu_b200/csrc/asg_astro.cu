@@ -59,6 +59,7 @@ struct StepArgs {
     double p, weight;
     const std::int64_t* step_base;  // device counter: step = *step_base + step_offset
     int step_offset;
+    std::int64_t i0;  // global index of the first cell of this launch (RNG streams)
 };
 
 template <bool kUniform, int kInput, bool kNoise>
@@ -67,7 +68,7 @@ __device__ __forceinline__ void advance_cell(const StepArgs& a, const AstroArray
                                              double& ip3, double& hh) {
     double in;
     if (kInput == kInputBernoulli) {
-        in = uniform_at(a.seed, static_cast<std::uint64_t>(i),
+        in = uniform_at(a.seed, static_cast<std::uint64_t>(a.i0 + i),
                         1000ULL + static_cast<std::uint64_t>(step)) < a.p
                  ? a.weight
                  : 0.0;
@@ -78,7 +79,7 @@ __device__ __forceinline__ void advance_cell(const StepArgs& a, const AstroArray
     if (kNoise) {
         noise = a.independent
                     ? a.noise_std * normal_clamped(a.noise_seed, a.noise_index * kStreamStride +
-                                                                     static_cast<std::uint64_t>(i))
+                                                                     static_cast<std::uint64_t>(a.i0 + i))
                     : a.shared_noise;
     }
     if (kUniform) {
@@ -209,9 +210,17 @@ struct AstroEngine {
     bool graph_uniform = true;
 
     ~AstroEngine() {
+        join_copies();
         if (graph) cudaGraphExecDestroy(graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (int c = 0; c < kMaxPieces; ++c) {
+            if (ev_in[c]) cudaEventDestroy(ev_in[c]);
+            if (ev_k[c]) cudaEventDestroy(ev_k[c]);
+            if (ev_out[c]) cudaEventDestroy(ev_out[c]);
+        }
+        if (h2d) cudaStreamDestroy(h2d);
+        if (d2h) cudaStreamDestroy(d2h);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -225,6 +234,39 @@ struct AstroEngine {
         return AstroArrays{Ca.as<double>(),     IP3.as<double>(),    h.as<double>(),
                            input.as<double>(),  Ca_tot.as<double>(), IP3_0.as<double>(),
                            tau.as<double>(),    inv_tau.as<double>(), delta.as<double>()};
+    }
+    // The same arrays from cell `off` on (per-cell parameters when present).
+    AstroArrays arrays_at(std::int64_t off) {
+        auto at = [off](DevBuf& b) { return b.get() ? b.as<double>() + off : nullptr; };
+        return AstroArrays{at(Ca), at(IP3), at(h), at(input), at(Ca_tot), at(IP3_0), at(tau),
+                           at(inv_tau), at(delta)};
+    }
+
+    // Drop-in copies and updates run as a pipeline over `pieces()` cell
+    // ranges: the input copy of range c+1 (host->device engine), the update
+    // of range c and the Ca copy of range c-1 (device->host engine) overlap.
+    // Events keep each range's order: input copy -> update -> Ca copy, and
+    // the next step's input copy and update after this step's update and Ca
+    // copy of the same range.
+    static constexpr int kMaxPieces = 8;
+    static constexpr std::int64_t kPieceCells = 1 << 18;
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ev_in[kMaxPieces] = {}, ev_k[kMaxPieces] = {}, ev_out[kMaxPieces] = {};
+    int pieces() const {
+        return static_cast<int>(std::max<std::int64_t>(
+            1, std::min<std::int64_t>(kMaxPieces, n / kPieceCells)));
+    }
+    // [begin, end) of range c: multiples of 64 cells (512-byte aligned).
+    std::int64_t piece_begin(int c) const {
+        return c == 0 ? 0 : ((n * c / pieces()) & ~static_cast<std::int64_t>(63));
+    }
+    std::int64_t piece_end(int c) const { return c + 1 == pieces() ? n : piece_begin(c + 1); }
+    // Later work on `stream` (state pulls, other updates) after every copy.
+    cudaError_t join_copies() {
+        cudaError_t e = cudaSuccess;
+        if (h2d) e = cudaStreamSynchronize(h2d);
+        if (e == cudaSuccess && d2h) e = cudaStreamSynchronize(d2h);
+        return e;
     }
 };
 
@@ -277,8 +319,15 @@ int asg_astro_create(uint32_t n, const double* Ca, const double* IP3, const doub
     if (st == ASG_OK) st = e->step_base.alloc(sizeof(std::int64_t));
     if (st == ASG_OK) {
         cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+        if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->h2d, cudaStreamNonBlocking);
+        if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->d2h, cudaStreamNonBlocking);
         if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev0);
         if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev1);
+        for (int c = 0; c < AstroEngine::kMaxPieces && ce == cudaSuccess; ++c) {
+            ce = cudaEventCreateWithFlags(&e->ev_in[c], cudaEventDisableTiming);
+            if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev_k[c], cudaEventDisableTiming);
+            if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev_out[c], cudaEventDisableTiming);
+        }
         if (ce != cudaSuccess) st = asg::cuda_fail(ce, "stream/event", __FILE__, __LINE__);
     }
     if (st != ASG_OK) {
@@ -307,6 +356,7 @@ int asg_astro_pull_state(asg_astro* s, double* Ca, double* IP3, double* h) {
     auto* e = reinterpret_cast<AstroEngine*>(s);
     const std::size_t bytes = static_cast<std::size_t>(e->n) * sizeof(double);
     if (bytes == 0) return ASG_OK;
+    ASG_CUDA(e->join_copies());
     ASG_CUDA(cudaMemcpyAsync(Ca, e->Ca.get(), bytes, cudaMemcpyDeviceToHost, e->stream));
     ASG_CUDA(cudaMemcpyAsync(IP3, e->IP3.get(), bytes, cudaMemcpyDeviceToHost, e->stream));
     ASG_CUDA(cudaMemcpyAsync(h, e->h.get(), bytes, cudaMemcpyDeviceToHost, e->stream));
@@ -319,10 +369,16 @@ int asg_astro_push_input(asg_astro* s, const double* ip3_input) {
     if (s == nullptr || ip3_input == nullptr)
         return asg::fail(ASG_ERR_ARG, "asg_astro_push_input: NULL argument");
     auto* e = reinterpret_cast<AstroEngine*>(s);
-    const std::size_t bytes = static_cast<std::size_t>(e->n) * sizeof(double);
-    if (bytes == 0) return ASG_OK;
-    ASG_CUDA(cudaMemcpyAsync(e->input.get(), ip3_input, bytes, cudaMemcpyHostToDevice,
-                             e->stream));
+    if (e->n == 0) return ASG_OK;
+    for (int c = 0; c < e->pieces(); ++c) {
+        const std::int64_t b = e->piece_begin(c), n = e->piece_end(c) - b;
+        // after the previous update consumed (zeroed) this range's input
+        ASG_CUDA(cudaStreamWaitEvent(e->h2d, e->ev_k[c], 0));
+        ASG_CUDA(cudaMemcpyAsync(e->input.as<double>() + b, ip3_input + b,
+                                 static_cast<std::size_t>(n) * sizeof(double),
+                                 cudaMemcpyHostToDevice, e->h2d));
+        ASG_CUDA(cudaEventRecord(e->ev_in[c], e->h2d));
+    }
     return ASG_OK;
 }
 
@@ -331,10 +387,16 @@ int asg_astro_pull_calcium(asg_astro* s, double* Ca) {
     if (s == nullptr || Ca == nullptr)
         return asg::fail(ASG_ERR_ARG, "asg_astro_pull_calcium: NULL argument");
     auto* e = reinterpret_cast<AstroEngine*>(s);
-    const std::size_t bytes = static_cast<std::size_t>(e->n) * sizeof(double);
-    if (bytes == 0) return ASG_OK;
-    ASG_CUDA(cudaMemcpyAsync(Ca, e->Ca.get(), bytes, cudaMemcpyDeviceToHost, e->stream));
-    ASG_CUDA(cudaStreamSynchronize(e->stream));
+    if (e->n == 0) return ASG_OK;
+    for (int c = 0; c < e->pieces(); ++c) {
+        const std::int64_t b = e->piece_begin(c), n = e->piece_end(c) - b;
+        ASG_CUDA(cudaStreamWaitEvent(e->d2h, e->ev_k[c], 0));  // after this range's update
+        ASG_CUDA(cudaMemcpyAsync(Ca + b, e->Ca.as<double>() + b,
+                                 static_cast<std::size_t>(n) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, e->d2h));
+        ASG_CUDA(cudaEventRecord(e->ev_out[c], e->d2h));
+    }
+    ASG_CUDA(cudaStreamSynchronize(e->d2h));
     return ASG_OK;
 }
 
@@ -364,8 +426,16 @@ int asg_astro_update(asg_astro* s, const double* consts, double h_step, int32_t 
     // The reference applies noise only when noise_std > 0 (astrocyte.cpp:
     // 313-322); otherwise the caller's shared value (0) enters the RHS.
     if (!(noise_std > 0.0)) a.independent = 0;
-    ASG_CUDA((asg::launch_astro<false, asg::kInputArray, true>(e->shape, e->sms, a,
-                                                                e->arrays(), e->stream)));
+    for (int c = 0; c < e->pieces(); ++c) {
+        const std::int64_t b = e->piece_begin(c);
+        ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_in[c], 0));   // this range's input
+        ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_out[c], 0));  // last Ca copy read it
+        a.n = e->piece_end(c) - b;
+        a.i0 = b;
+        ASG_CUDA((asg::launch_astro<false, asg::kInputArray, true>(e->shape, e->sms, a,
+                                                                    e->arrays_at(b), e->stream)));
+        ASG_CUDA(cudaEventRecord(e->ev_k[c], e->stream));
+    }
     ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
     e->last_kernels = 1;
     return ASG_OK;
@@ -388,6 +458,7 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
         e->last_kernels = 0;
         return ASG_OK;
     }
+    ASG_CUDA(e->join_copies());
     asg::StepArgs a;
     std::memset(&a, 0, sizeof a);
     a.n = e->n;
@@ -478,6 +549,7 @@ extern "C" int asg_astro_autotune(asg_astro* s, const double* consts, double h_s
     auto* e = reinterpret_cast<AstroEngine*>(s);
     if (e->n == 0) return ASG_OK;
     const std::size_t bytes = static_cast<std::size_t>(e->n) * sizeof(double);
+    ASG_CUDA(e->join_copies());
     // Scratch copies of the state: the trials advance these, not the handle's.
     asg::DevBuf ca, ip3, h;
     ASG_TRY(ca.alloc(bytes, false));

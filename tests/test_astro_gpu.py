@@ -64,3 +64,33 @@ def test_drop_in_backend_per_cell_params_and_input():
         assert np.array_equal(gpu.pull_calcium(), rCa)
     gCa, gIP3, gh = gpu.destroy()
     assert np.array_equal(gIP3, rIP3) and np.array_equal(gh, rh)
+
+
+def test_drop_in_backend_pipelined_cell_ranges():
+    """Large handles copy and update in up to eight cell ranges whose copies
+    overlap the updates; the result is the oracle's, bit for bit, including
+    at range boundaries, on consecutive steps and when the caller reuses one
+    input buffer."""
+    rng = np.random.default_rng(5)
+    n = 3 * (1 << 18) + 77  # three ranges, the last one ragged
+    w = ScalingWorkload(n)
+    Ca, IP3, h = w.initial_state()
+    Ca_tot = w.Ca_tot * (1 + 0.05 * rng.standard_normal(n))
+    IP3_0 = w.IP3_0 * (1 + 0.05 * rng.standard_normal(n))
+    tau = w.tau_IP3 * (1 + 0.05 * rng.standard_normal(n))
+    delta = w.delta_IP3 * (1 + 0.05 * rng.standard_normal(n))
+    gpu = AstroBackend(Ca, IP3, h, Ca_tot, IP3_0, tau, delta)
+    rCa, rIP3, rh = Ca.copy(), IP3.copy(), h.copy()
+    lib = ref.ref()
+    inp = np.empty(n)
+    for step in range(4):
+        inp[:] = np.where(rng.random(n) < 0.3, rng.random(n), 0.0)
+        gpu.push_input(inp)
+        gpu.update(w.consts, w.h_step, 2)
+        lib.ref_astro_advance(ref._dp(w.consts), n, ref._dp(Ca_tot), ref._dp(IP3_0),
+                              ref._dp(tau), ref._dp(delta), ref._dp(inp), None, w.h_step, 2,
+                              ref._dp(rCa), ref._dp(rIP3), ref._dp(rh))
+        if step % 2:
+            assert np.array_equal(gpu.pull_calcium(), rCa), step
+    gCa, gIP3, gh = gpu.destroy()
+    assert np.array_equal(gCa, rCa) and np.array_equal(gIP3, rIP3) and np.array_equal(gh, rh)

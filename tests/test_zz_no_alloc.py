@@ -57,6 +57,43 @@ def test_noalloc_matches_regular_entry_point_twice():
     regular.destroy()
 
 
+def test_pipelined_ranges_with_noise_match_single_launch():
+    """The regular entry point splits a large handle into cell ranges, each
+    launch offset to its first cell; with independent noise every cell must
+    still draw its own stream, as the single-launch no-alloc call does."""
+    import torch
+    rng = np.random.default_rng(12)
+    n = 3 * (1 << 18) + 77
+    w = ScalingWorkload(n)
+    Ca, IP3, h = w.initial_state()
+    Ca_tot = w.Ca_tot * (1 + 0.05 * rng.standard_normal(n))
+    IP3_0 = w.IP3_0 * (1 + 0.05 * rng.standard_normal(n))
+    tau = w.tau_IP3 * (1 + 0.05 * rng.standard_normal(n))
+    delta = w.delta_IP3 * (1 + 0.05 * rng.standard_normal(n))
+    regular = AstroBackend(Ca, IP3, h, Ca_tot, IP3_0, tau, delta)
+    d = {k: dev(v) for k, v in dict(Ca=Ca, IP3=IP3, h=h, Ca_tot=Ca_tot, IP3_0=IP3_0, tau=tau,
+                                       delta=delta, inp=np.zeros(n)).items()}
+    lib = _lib.load()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for step in range(3):
+        inp = np.where(rng.random(n) < 0.3, rng.random(n), 0.0)
+        regular.push_input(inp)
+        regular.update(w.consts, w.h_step, 2, noise_std=0.05, independent=True,
+                       noise_seed=77, noise_index=step)
+        d["inp"].copy_(torch.from_numpy(inp))
+        st = lib.asg_astro_update_noalloc(
+            n, *[C.c_void_p(d[k].data_ptr()) for k in ("Ca", "IP3", "h", "inp", "Ca_tot",
+                                                         "IP3_0", "tau", "delta")],
+            _lib.dptr(w.consts), w.h_step, 2, 0.05, 1, 0.0, 77, step, stream)
+        assert st == 0, lib.asg_last_error()
+    torch.cuda.synchronize()
+    rCa, rIP3, rh = regular.pull_state()
+    assert np.array_equal(d["Ca"].cpu().numpy(), rCa)
+    assert np.array_equal(d["IP3"].cpu().numpy(), rIP3)
+    assert np.array_equal(d["h"].cpu().numpy(), rh)
+    regular.destroy()
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     lib = _lib.load()
     null = C.c_void_p(16)  # never dereferenced: the size check comes first
