@@ -77,7 +77,7 @@ AstroK make_astro_k(const asg_astro_params& a, double h, int substeps) {
 // target's words marks an arrival on that edge.
 struct InRingHost {
     std::vector<std::uint32_t> wbase;
-    std::vector<unsigned long long> edge;  // bit | target << 32 | summary bit << 58
+    std::vector<unsigned long long> edge;  // bit | target << 32 | dense << 57 | summary bit << 58
     std::uint32_t words = 0;
 };
 
@@ -101,7 +101,10 @@ InRingHost make_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std:
             const std::uint32_t nw = r.wbase[t + 1] - r.wbase[t];
             const std::uint32_t G = (nw + 63) / 64;
             const unsigned long long bit = static_cast<unsigned long long>(r.wbase[t]) * 32 + p;
-            r.edge[e] = bit | (static_cast<unsigned long long>(t) << 32) |
+            // A target of at most 32 words reads all its words at once and
+            // never its summary: its pushes skip the summary update.
+            const unsigned long long dense = nw <= 32 ? 1ull : 0ull;
+            r.edge[e] = bit | (static_cast<unsigned long long>(t) << 32) | (dense << 57) |
                         (static_cast<unsigned long long>((p / 32) / G) << 58);
         }
     }
@@ -364,7 +367,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     if (!delay_ok(d.d_e_steps) || !delay_ok(d.d_i_steps) || !delay_ok(d.d_a2n_steps))
         return fail(ASG_ERR_ARG, "delays must be at least one step");
     if (NA >= (1u << 24)) return fail(ASG_ERR_UNSUPPORTED, "at most 2^24-1 astrocytes");
-    if (NE + NI >= (1u << 26)) return fail(ASG_ERR_UNSUPPORTED, "at most 2^26-1 neurons");
+    if (NE + NI >= (1u << 25)) return fail(ASG_ERR_UNSUPPORTED, "at most 2^25-1 neurons");
     if (N > 0 && (d.V_reset == nullptr || d.b == nullptr))
         return fail(ASG_ERR_ARG, "per-cell V_reset and b are required");
     if (first < 0 || end < first) return fail(ASG_ERR_ARG, "bad step range");

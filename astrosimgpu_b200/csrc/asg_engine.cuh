@@ -27,8 +27,10 @@
 // the word group holding it (64-bit summary per target and slot).  The
 // target, when the slot arrives, reads its counter; for up to kListCap
 // arrivals it loads the list in one batch and sorts it by bit; beyond that it
-// also visits the non-empty words its summary names, walking their set bits
-// in ascending order and merging them with the sorted list.  Either way the
+// also walks the set bits of its bitmap words in ascending order, merging
+// them with the sorted list (a target of at most 32 words loads all of them
+// in one batch; a larger one visits the non-empty words its summary names).
+// Either way the
 // values are added left to right in ascending bit order: the reference's
 // IEEE operations in the reference's order, hence bitwise equal, for any
 // number of coincident spikes and any interleaving of the pushes.  Reading
@@ -80,14 +82,15 @@ constexpr int kSicRing = 32;       // SIC value slots of an instance with side b
 
 struct InRing {
     const std::uint32_t* wbase;   // [n_targets+1] first bitmap word of each target
-    // [E] per OUT-edge (source CSR order): bit index | target << 32 | summary
-    // bit << 58 -- one 8-byte load gives everything a push needs.
+    // [E] per OUT-edge (source CSR order): bit index | target << 32 | dense
+    // << 57 (target of at most 32 words: no summary) | summary bit << 58 --
+    // one 8-byte load gives everything a push needs.
     const unsigned long long* edge;
     std::uint32_t* cnt;           // [slots][n_targets] arrivals pushed into the slot
     std::uint32_t* lbit;          // [slots][n_targets][kListCap] bits of the first arrivals
     double* lval;                 // [slots][n_targets][kListCap] their values
     std::uint32_t* bits;          // [slots][words] bitmaps of the later arrivals
-    unsigned long long* sum;      // [slots][n_targets] non-empty word groups
+    unsigned long long* sum;      // [slots][n_targets] non-empty word groups (targets of > 32 words)
     double* vals;                 // [slots][words*32] value at each set bit
     std::uint32_t words;          // total bitmap words of one slot
     std::uint32_t n_targets;

@@ -163,6 +163,82 @@ __device__ __forceinline__ double accumulate(double acc, double v, bool sub) {
     return sub ? acc - v : acc + v;
 }
 
+// merge_overflow for a target of at most 32 bitmap words (in-degree <= 1024):
+// every word in one batch of loads (its pushes keep no summary), then the set bits in
+// ascending order in passes of 8 value loads.  The words sit in a local
+// array (the walk indexes it at run time); the pass's value loads are issued
+// at the same point of the code by all lanes, as in merge_overflow.  (Passes
+// of 12 or 16 loads measured slower: the larger register footprint of this
+// out-of-line call costs the step kernel spills on its common path.)
+__device__ __forceinline__ double merge_dense(std::uint32_t* bits, const double* vals,
+                                              std::uint32_t w0,
+                                              std::uint32_t nw, bool sub, std::uint32_t l0,
+                                              std::uint32_t l1, std::uint32_t l2,
+                                              std::uint32_t l3, double v0, double v1, double v2,
+                                              double v3) {
+    std::uint32_t wv[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k)
+        wv[k] = static_cast<std::uint32_t>(k) < nw ? __ldcg(bits + w0 + k) : 0u;
+    std::uint32_t live = 0;  // words with bits not yet taken
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        if (wv[k] != 0) {
+            live |= 1u << k;
+            bits[w0 + k] = 0;
+        }
+    }
+    double acc = 0.0;
+    std::uint32_t cw = 0, ck = 0;  // bits left in the current word, its index
+    for (;;) {
+        std::uint32_t idx[8];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            if (cw == 0 && live != 0) {
+                ck = static_cast<std::uint32_t>(__ffs(live) - 1);
+                live &= live - 1;
+                cw = wv[ck];
+            }
+            if (cw != 0) {
+                idx[s] = (w0 + ck) * 32 + static_cast<std::uint32_t>(__ffs(cw) - 1);
+                cw &= cw - 1;
+            } else {
+                idx[s] = kNoBit;
+            }
+        }
+        if (idx[0] == kNoBit) break;
+        double v[8];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) v[s] = idx[s] != kNoBit ? __ldcg(vals + idx[s]) : 0.0;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            if (idx[s] == kNoBit) break;
+            while (l0 < idx[s]) {  // list entries that precede this bit
+                acc = accumulate(acc, v0, sub);
+                l0 = l1;
+                v0 = v1;
+                l1 = l2;
+                v1 = v2;
+                l2 = l3;
+                v2 = v3;
+                l3 = kNoBit;
+            }
+            acc = accumulate(acc, v[s], sub);
+        }
+    }
+    while (l0 != kNoBit) {
+        acc = accumulate(acc, v0, sub);
+        l0 = l1;
+        v0 = v1;
+        l1 = l2;
+        v1 = v2;
+        l2 = l3;
+        v2 = v3;
+        l3 = kNoBit;
+    }
+    return acc;
+}
+
 // More than kListCap arrivals: the first kListCap (sorted, l0 < l1 < l2 <
 // l3) are merged in bit order with the later ones, which sit in the
 // target's bitmap words (visited through the summary).  Loads go out in
@@ -178,11 +254,13 @@ __device__ __noinline__ double merge_overflow(const InRing& R, std::uint32_t slo
                                               std::uint32_t l3, double v0, double v1, double v2,
                                               double v3) {
     unsigned long long* sp = R.sum + static_cast<std::size_t>(slot) * R.n_targets + t;
-    unsigned long long groups = __ldcg(sp);
-    *sp = 0;
     std::uint32_t* bits = R.bits + static_cast<std::size_t>(slot) * R.words;
     const double* vals = R.vals + static_cast<std::size_t>(slot) * R.words * 32;
     const std::uint32_t w0 = R.wbase[t], nw = R.wbase[t + 1] - w0;
+    if (nw <= 32)
+        return merge_dense(bits, vals, w0, nw, sub, l0, l1, l2, l3, v0, v1, v2, v3);
+    unsigned long long groups = __ldcg(sp);
+    *sp = 0;
     const std::uint32_t G = (nw + 63) >> 6;  // words per summary bit
     double acc = 0.0;
     std::uint32_t q[8], wv[8];
@@ -289,13 +367,14 @@ __device__ __forceinline__ double sum_arrivals(const InRing& R, std::uint32_t sl
     return acc;
 }
 
-// One arrival on the edge with packed word `pe` (bit | target << 32 |
-// summary bit << 58): a ticket from the target's counter decides between
-// the short list and the bitmap.
+// One arrival on the edge with packed word `pe` (bit | target << 32 | dense
+// << 57 | summary bit << 58): a ticket from the target's counter decides
+// between the short list and the bitmap; the summary is kept only for
+// targets of more than 32 words.
 __device__ __forceinline__ void push_edge(const InRing& R, std::uint32_t slot,
                                           unsigned long long pe, double value) {
     const std::uint32_t b = static_cast<std::uint32_t>(pe);
-    const std::uint32_t t = static_cast<std::uint32_t>(pe >> 32) & 0x3FFFFFFu;
+    const std::uint32_t t = static_cast<std::uint32_t>(pe >> 32) & 0x1FFFFFFu;
     const std::size_t ts = static_cast<std::size_t>(slot) * R.n_targets + t;
     const std::uint32_t k = atomicAdd(R.cnt + ts, 1u);
     if (k < static_cast<std::uint32_t>(kListCap)) {
@@ -305,7 +384,7 @@ __device__ __forceinline__ void push_edge(const InRing& R, std::uint32_t slot,
         const std::uint32_t g = static_cast<std::uint32_t>(pe >> 58);
         R.vals[static_cast<std::size_t>(slot) * R.words * 32 + b] = value;
         atomicOr(R.bits + static_cast<std::size_t>(slot) * R.words + (b >> 5), 1u << (b & 31));
-        atomicOr(R.sum + ts, 1ull << g);
+        if (((pe >> 57) & 1ull) == 0) atomicOr(R.sum + ts, 1ull << g);
     }
 }
 
@@ -637,7 +716,7 @@ constexpr int kPushBatch = 256;
 __device__ void push_spikes(const InstDev& I, const StepInfo& S, unsigned long long packed,
                             std::uint32_t rank, std::uint32_t nranks) {
     __shared__ std::uint32_t s_off[kPushBatch + 1], s_src[kPushBatch], s_r0[kPushBatch],
-        s_len0[kPushBatch];
+        s_len0[kPushBatch], s_r1[kPushBatch];
     __shared__ double s_v[2 * kPushBatch];
     const std::uint32_t n = static_cast<std::uint32_t>(packed >> 40);
     const std::uint32_t total = static_cast<std::uint32_t>(packed & 0xFFFFFFFFFFull);
@@ -656,6 +735,7 @@ __device__ void push_spikes(const InstDev& I, const StepInfo& S, unsigned long l
             s_off[i] = m.y;
             s_r0[i] = m.z;
             s_len0[i] = m.w;
+            s_r1[i] = m.x < I.NE ? __ldg(I.n2a_rs + m.x) : 0u;  // astrocyte row of the source
             s_v[2 * i] = v.x;
             s_v[2 * i + 1] = v.y;
         }
@@ -664,22 +744,47 @@ __device__ void push_spikes(const InstDev& I, const StepInfo& S, unsigned long l
         __syncthreads();
         // The list order is the atomic order, so offsets ascend along it.
         const std::uint32_t x0 = s_off[0], x1 = s_off[nb];
-#pragma unroll 4
-        for (std::uint32_t x = x0 + gtid; x < x1; x += stride) {
-            std::uint32_t lo = 0, hi = nb;  // last entry with s_off <= x
-            while (hi - lo > 1) {
-                const std::uint32_t mid = (lo + hi) >> 1;
-                if (s_off[mid] <= x) lo = mid; else hi = mid;
+        // Groups of kPushGroup edges per thread: every edge word of the group
+        // is loaded before the group's tickets are taken, so a thread waits
+        // one round trip for its edges and one for its tickets per group.
+        constexpr int kPushGroup = 4;
+        for (std::uint32_t xg = x0 + gtid; xg < x1; xg += kPushGroup * stride) {
+            unsigned long long pe[kPushGroup];
+            double val[kPushGroup];
+            int which[kPushGroup];  // 0 inh, 1 exc, 2 astrocyte, -1 none
+#pragma unroll
+            for (int u = 0; u < kPushGroup; ++u) {
+                const std::uint32_t x = xg + static_cast<std::uint32_t>(u) * stride;
+                which[u] = -1;
+                pe[u] = 0;
+                val[u] = 0.0;
+                if (x < x1) {
+                    std::uint32_t lo = 0, hi = nb;  // last entry with s_off <= x
+                    while (hi - lo > 1) {
+                        const std::uint32_t mid = (lo + hi) >> 1;
+                        if (s_off[mid] <= x) lo = mid; else hi = mid;
+                    }
+                    const std::uint32_t k = x - s_off[lo];
+                    if (s_src[lo] >= I.NE) {
+                        which[u] = 0;
+                        pe[u] = __ldg(I.ring_in.edge + s_r0[lo] + k);
+                        val[u] = s_v[2 * lo];
+                    } else if (k < s_len0[lo]) {
+                        which[u] = 1;
+                        pe[u] = __ldg(I.ring_ex.edge + s_r0[lo] + k);
+                        val[u] = s_v[2 * lo];
+                    } else {
+                        which[u] = 2;
+                        pe[u] = __ldg(I.ring_as.edge + s_r1[lo] + (k - s_len0[lo]));
+                        val[u] = s_v[2 * lo + 1];
+                    }
+                }
             }
-            const std::uint32_t j = s_src[lo];
-            const std::uint32_t k = x - s_off[lo];
-            if (j >= I.NE) {
-                push_edge(I.ring_in, as_i, __ldg(I.ring_in.edge + s_r0[lo] + k), s_v[2 * lo]);
-            } else if (k < s_len0[lo]) {
-                push_edge(I.ring_ex, as_e, __ldg(I.ring_ex.edge + s_r0[lo] + k), s_v[2 * lo]);
-            } else {
-                push_edge(I.ring_as, as_e, __ldg(I.ring_as.edge + I.n2a_rs[j] + (k - s_len0[lo])),
-                          s_v[2 * lo + 1]);
+#pragma unroll
+            for (int u = 0; u < kPushGroup; ++u) {
+                if (which[u] == 0) push_edge(I.ring_in, as_i, pe[u], val[u]);
+                else if (which[u] == 1) push_edge(I.ring_ex, as_e, pe[u], val[u]);
+                else if (which[u] == 2) push_edge(I.ring_as, as_e, pe[u], val[u]);
             }
         }
     }
