@@ -148,7 +148,8 @@ struct InstDev {
     // the slot being appended to (atomics) and the slot being read by every
     // block must not share an L2 sector, or the reads queue behind the atomics.
     unsigned long long* spk_packed;
-    std::uint32_t* spk_meta;           // [3][N][4]: source, edge offset, row0 start, row0 length
+    std::uint32_t* spk_meta;           // [3][N][4]: n2a row start (~0: inhibitory source),
+                                       // edge offset, row0 start, row0 length
     double* spk_val;                   // [3][N][2]: exc or inh set value, n2a value
     // SIC: sliced ELL over virtual targets v = part * sic_npad + target,
     // factors per emission slot, partial sums between parts, final values.

@@ -654,12 +654,15 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
                 exc ? (I.stp_on ? I.w_e * x * u : I.w_e) : (I.stp_on ? I.w_i * x * u : I.w_i);
             const double v1 = exc ? (I.stp_on ? I.w_n2a * x * u : I.w_n2a) : 0.0;
             if (I.deferred_push) {
+                // n2a row start of an excitatory source (~0: inhibitory),
+                // loaded while the append's atomic is in flight
+                const std::uint32_t r1 = exc ? __ldg(I.n2a_rs + c) : kNoBit;
                 const unsigned long long old = atomicAdd(
                     I.spk_packed + S.ls * kHeaderStride,
                     (1ull << 40) | static_cast<unsigned long long>(len0 + len1));
                 const std::size_t o = static_cast<std::size_t>(S.ls) * I.N + (old >> 40);
                 *reinterpret_cast<uint4*>(I.spk_meta + 4 * o) =
-                    make_uint4(c, static_cast<std::uint32_t>(old & 0xFFFFFFFFFFull), r0, len0);
+                    make_uint4(r1, static_cast<std::uint32_t>(old & 0xFFFFFFFFFFull), r0, len0);
                 *reinterpret_cast<double2*>(I.spk_val + 2 * o) = make_double2(v0, v1);
             } else {
                 s_val[threadIdx.x * 2 + 0] = v0;
@@ -715,8 +718,8 @@ constexpr int kPushBatch = 256;
 // x % (nranks * blockDim.x) of the participants.
 __device__ void push_spikes(const InstDev& I, const StepInfo& S, unsigned long long packed,
                             std::uint32_t rank, std::uint32_t nranks) {
-    __shared__ std::uint32_t s_off[kPushBatch + 1], s_src[kPushBatch], s_r0[kPushBatch],
-        s_len0[kPushBatch], s_r1[kPushBatch];
+    __shared__ std::uint32_t s_off[kPushBatch + 1], s_r0[kPushBatch], s_len0[kPushBatch],
+        s_r1[kPushBatch];
     __shared__ double s_v[2 * kPushBatch];
     const std::uint32_t n = static_cast<std::uint32_t>(packed >> 40);
     const std::uint32_t total = static_cast<std::uint32_t>(packed & 0xFFFFFFFFFFull);
@@ -731,11 +734,10 @@ __device__ void push_spikes(const InstDev& I, const StepInfo& S, unsigned long l
             const std::size_t o = base + b0 + i;
             const uint4 m = __ldcg(reinterpret_cast<const uint4*>(I.spk_meta + 4 * o));
             const double2 v = __ldcg(reinterpret_cast<const double2*>(I.spk_val + 2 * o));
-            s_src[i] = m.x;
+            s_r1[i] = m.x;  // n2a row start; kNoBit marks an inhibitory source
             s_off[i] = m.y;
             s_r0[i] = m.z;
             s_len0[i] = m.w;
-            s_r1[i] = m.x < I.NE ? __ldg(I.n2a_rs + m.x) : 0u;  // astrocyte row of the source
             s_v[2 * i] = v.x;
             s_v[2 * i + 1] = v.y;
         }
@@ -765,7 +767,7 @@ __device__ void push_spikes(const InstDev& I, const StepInfo& S, unsigned long l
                         if (s_off[mid] <= x) lo = mid; else hi = mid;
                     }
                     const std::uint32_t k = x - s_off[lo];
-                    if (s_src[lo] >= I.NE) {
+                    if (s_r1[lo] == kNoBit) {
                         which[u] = 0;
                         pe[u] = __ldg(I.ring_in.edge + s_r0[lo] + k);
                         val[u] = s_v[2 * lo];
