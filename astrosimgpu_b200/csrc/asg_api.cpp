@@ -26,6 +26,18 @@ EngineConfig config_from(const asg_engine_opts* o) {
     return c;
 }
 
+// Default chunk of a single network: about 2^23 neuron-steps per chunk, a
+// power of two in [32, 512].  Longer chunks cost fewer chunk boundaries (a
+// descriptor copy, a counter copy and reset, a graph launch and a first step
+// without early launch: ~20 us of device time each), while the per-chunk
+// spike log (N * chunk / 8 entries, two pinned buffers) stays at most 8 MB.
+int default_chunk(std::uint64_t n_neurons) {
+    const std::uint64_t want = (1ull << 23) / std::max<std::uint64_t>(n_neurons, 1);
+    int c = 32;
+    while (c < 512 && static_cast<std::uint64_t>(c) * 2 <= want) c *= 2;
+    return c;
+}
+
 namespace {
 
 int fetch_spikes_from(Instance* I, int64_t* steps, uint32_t* sources, int64_t cap,
@@ -148,7 +160,7 @@ int autotune_engine(Engine& e, int32_t steps, asg_engine_opts* chosen) {
     int best_block = block0, best_chunk = chunk0, best_mode = mode0;
     double best = 1e300;
     for (int mode : {1, 2}) {
-        for (int chunk : {32, 64, 128}) {
+        for (int chunk : {32, 64, 128, 256, 512}) {  // up to the chunk the instances were sized for
             if (e.set_chunk(chunk) != ASG_OK) continue;
             for (int block : {128, 256, 512}) {
                 ASG_TRY(e.set_block(block));
@@ -202,7 +214,10 @@ int asg_create(const asg_network_desc* desc, const asg_record_opts* rec,
     if (desc == nullptr || out == nullptr) return asg::fail(ASG_ERR_ARG, "asg_create: NULL argument");
     *out = nullptr;
     auto h = std::make_unique<NetworkHandle>();
-    h->eng = std::make_unique<Engine>(asg::config_from(opts));
+    asg::EngineConfig cfg = asg::config_from(opts);
+    if (opts == nullptr || opts->chunk_steps <= 0)
+        cfg.chunk_steps = asg::default_chunk(static_cast<std::uint64_t>(desc->n_exc) + desc->n_inh);
+    h->eng = std::make_unique<Engine>(cfg);
     ASG_TRY(h->eng->init());
     ASG_TRY(h->eng->add(*desc, rec, 0, INT64_MAX, true, &h->id));
     *out = reinterpret_cast<asg_network*>(h.release());

@@ -266,7 +266,7 @@ Engine::Engine(const EngineConfig& c) : cfg(c) {}
 
 Engine::~Engine() {
     if (stream) cudaStreamSynchronize(stream);
-    if (graph) cudaGraphExecDestroy(graph);
+    drop_graphs();
     for (int p = 0; p < 2; ++p) {
         if (h_insts[p]) cudaFreeHost(h_insts[p]);
         if (h_stats[p]) cudaFreeHost(h_stats[p]);
@@ -683,10 +683,7 @@ int Engine::set_chunk(int chunk) {
 int Engine::rebuild() {
     ASG_TRY(finish_pending());
     ASG_CUDA(cudaStreamSynchronize(stream));
-    if (graph) {
-        cudaGraphExecDestroy(graph);
-        graph = nullptr;
-    }
+    drop_graphs();
     const int B = cfg.block;
     work.clear();
     order.clear();
@@ -770,29 +767,57 @@ int Engine::rebuild() {
                                  side_work.size() * sizeof(Work), cudaMemcpyHostToDevice, stream));
     ASG_CUDA(cudaMemsetAsync(d_stats.get(), 0, cap_insts * 8 * sizeof(unsigned long long), stream));
     ASG_CUDA(cudaStreamSynchronize(stream));
-    graph_steps = 0;
     persistent_grid = 0;
     if (cfg.use_graphs == 2 && !work.empty()) {
         const int cap = persistent_blocks(B);
         if (cap <= 0) return fail(ASG_ERR_CUDA, "persistent kernel: no co-resident blocks");
         persistent_grid = std::min<int>(cap, static_cast<int>(work.size()));
     }
-    if ((cfg.use_graphs == 0 || cfg.use_graphs == 1) && !work.empty()) {
-        cudaGraph_t g = nullptr;
-        ASG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        const cudaError_t le = issue_steps(cfg.chunk_steps);
-        const cudaError_t ce = cudaStreamEndCapture(stream, &g);
-        if (le != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            return cuda_fail(le, "step launch (capture)", __FILE__, __LINE__);
-        }
-        if (ce != cudaSuccess) return cuda_fail(ce, "graph capture", __FILE__, __LINE__);
-        const cudaError_t ci = cudaGraphInstantiate(&graph, g, 0);
-        cudaGraphDestroy(g);
-        if (ci != cudaSuccess) return cuda_fail(ci, "graph instantiate", __FILE__, __LINE__);
-        graph_steps = cfg.chunk_steps;
-    }
     dirty = false;
+    if (graph_mode() && !work.empty()) ASG_TRY(capture_graph(cfg.chunk_steps));
+    return ASG_OK;
+}
+
+void Engine::drop_graphs() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    graphs.clear();
+}
+
+cudaGraphExec_t Engine::find_graph(int steps) {
+    for (std::size_t i = 0; i < graphs.size(); ++i) {
+        if (graphs[i].first != steps) continue;
+        std::rotate(graphs.begin(), graphs.begin() + static_cast<std::ptrdiff_t>(i),
+                    graphs.begin() + static_cast<std::ptrdiff_t>(i) + 1);
+        return graphs.front().second;
+    }
+    return nullptr;
+}
+
+// The graph of a chunk of `steps` steps, captured unless cached.  Capturing
+// waits for the chunks in flight, so the streams it records on are idle.
+int Engine::capture_graph(int steps) {
+    if (find_graph(steps) != nullptr) return ASG_OK;
+    ASG_TRY(finish_pending());
+    ASG_CUDA(cudaStreamSynchronize(stream));
+    if (side) ASG_CUDA(cudaStreamSynchronize(side));
+    cudaGraph_t g = nullptr;
+    ASG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t le = issue_steps(steps);
+    const cudaError_t ce = cudaStreamEndCapture(stream, &g);
+    if (le != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(le, "step launch (capture)", __FILE__, __LINE__);
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "graph capture", __FILE__, __LINE__);
+    cudaGraphExec_t x = nullptr;
+    const cudaError_t ci = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (ci != cudaSuccess) return cuda_fail(ci, "graph instantiate", __FILE__, __LINE__);
+    if (graphs.size() == kMaxGraphs) {
+        cudaGraphExecDestroy(graphs.back().second);
+        graphs.pop_back();
+    }
+    graphs.insert(graphs.begin(), {steps, x});
     return ASG_OK;
 }
 
@@ -891,8 +916,8 @@ int Engine::launch_chunk(int parity, int steps) {
                                          stream));
         ASG_CUDA(cudaMemcpyAsync(h_barrier_err[parity], &d_barrier.as<GridBarrier>()->error,
                                  sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
-    } else if (graph != nullptr && steps == graph_steps) {
-        ASG_CUDA(cudaGraphLaunch(graph, stream));
+    } else if (cudaGraphExec_t g = graph_mode() ? find_graph(steps) : nullptr) {
+        ASG_CUDA(cudaGraphLaunch(g, stream));
     } else {
         ASG_CUDA(issue_steps(steps));
     }
@@ -1013,14 +1038,36 @@ int Engine::run(std::int64_t n_steps) {
         saved_end[s] = insts[s]->end;
         insts[s]->end = target[s];
     }
-    ASG_CUDA(cudaEventRecord(ev_start, stream));
+    // Equal chunks: the l steps left run as ceil(l / chunk_steps) chunks of
+    // ceil(l / c) or ceil(l / c) - 1 steps.  Their graphs (at most two
+    // lengths) are captured before the timed region; on a failure every
+    // instance's window is restored before returning.
+    auto left = [&]() {
+        std::int64_t m = 0;
+        for (auto& p : insts) m = std::max<std::int64_t>(m, p->end - p->step);
+        return m;
+    };
+    auto next_chunk = [&](std::int64_t l) {
+        const std::int64_t c = (l + cfg.chunk_steps - 1) / cfg.chunk_steps;
+        return (l + c - 1) / c;
+    };
     int st = ASG_OK;
-    for (;;) {
-        bool any = false;
-        for (auto& p : insts) any = any || !p->done();
-        if (!any) break;
-        st = run_chunk(cfg.chunk_steps);
-        if (st != ASG_OK) break;
+    if (graph_mode() && !work.empty()) {
+        for (std::int64_t l = left(), prev = 0; l > 0 && st == ASG_OK; l -= prev) {
+            const std::int64_t a = next_chunk(l);
+            if (a != prev) st = capture_graph(static_cast<int>(a));
+            prev = a;
+        }
+    }
+    if (st == ASG_OK) {
+        const cudaError_t e = cudaEventRecord(ev_start, stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "event record", __FILE__, __LINE__);
+    }
+    for (; st == ASG_OK;) {
+        const std::int64_t l = left();
+        if (l <= 0) break;
+        st = run_chunk(next_chunk(l));
+        if (st == ASG_OK && left() == l) break;  // nothing to launch (no work items)
     }
     if (st == ASG_OK) st = finish_pending();
     for (std::size_t s = 0; s < insts.size(); ++s) insts[s]->end = saved_end[s];

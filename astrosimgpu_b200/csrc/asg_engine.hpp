@@ -77,7 +77,9 @@ public:
     static int footprint(const asg_network_desc& d, int chunk_steps, std::uint64_t* bytes);
 
     // Runs chunks until every instance advanced by n_steps (or reached its
-    // end).  Outputs are gathered into each Instance.
+    // end).  Outputs are gathered into each Instance.  A call runs as equal
+    // chunks of at most chunk_steps (1000 steps at chunk 512: two of 500),
+    // each one captured graph.
     int run(std::int64_t n_steps);
     // One chunk of up to chunk_steps (serving loop granularity).
     int run_chunk(std::int64_t max_steps);
@@ -127,8 +129,14 @@ private:
     std::size_t cap_insts = 0;
     std::vector<Work> work;
     std::vector<int> order;  // instance index per device slot
-    cudaGraphExec_t graph = nullptr;
-    int graph_steps = 0;
+    // Captured chunk graphs by length, most recently used first: the
+    // chunk_steps graph and the lengths run() splits its calls into.
+    static constexpr std::size_t kMaxGraphs = 4;
+    std::vector<std::pair<int, cudaGraphExec_t>> graphs;
+    bool graph_mode() const { return cfg.use_graphs == 0 || cfg.use_graphs == 1; }
+    cudaGraphExec_t find_graph(int steps);
+    int capture_graph(int steps);
+    void drop_graphs();
     bool dirty = true;
     // side-stream SIC batches (instances with InstDev::sic_side)
     static constexpr int kSideEvents = 8;

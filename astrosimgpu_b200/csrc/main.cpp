@@ -34,7 +34,7 @@ void usage(const char* argv0) {
               << "  -t, --sim-time MS     recorded duration       [from config]\n"
               << "  -p, --pre-time MS     discarded transient     [from config]\n"
               << "  -a, --astrocytes N    override the astrocyte count [from config]\n"
-              << "      --chunk N         steps per captured CUDA graph [64]\n"
+              << "      --chunk N         steps per captured CUDA graph [by network size]\n"
               << "      --no-analysis     skip the post-run summary\n"
               << "  -h, --help            show this message\n";
 }
@@ -54,7 +54,7 @@ int main(int argc, char** argv) {
     long long seed = -1, astro = -1;
     double sim = -1.0, pre = -1.0;
     bool analysis = true;
-    int chunk = 64;
+    int chunk = 0;  // 0: the engine's default for the network size
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         auto next = [&]() -> std::string {

@@ -30,7 +30,8 @@ def main(argv=None) -> int:
     ap.add_argument("--save", help="write a checkpoint after the steps")
     ap.add_argument("--load", help="resume from a checkpoint before the steps")
     ap.add_argument("--plain", action="store_true", help="one launch per step, no graphs")
-    ap.add_argument("--chunk", type=int, default=64, help="steps per chunk")
+    ap.add_argument("--chunk", type=int, default=0,
+                    help="steps per chunk (0: the engine's default for the network size)")
     args = ap.parse_args(argv)
 
     path = args.config if os.path.exists(args.config) else config_path(args.config)

@@ -283,7 +283,6 @@ def bench_network(name="paper_sparse_dt005", calls=20, steady_calls=5, **opts):
     t0 = time.perf_counter()
     m = Model(config_path(name), pre_time=0.0)
     build_s = time.perf_counter() - t0
-    opts.setdefault("chunk_steps", 128)
     net = Network(m, record=_lib.RecordOpts(0, 10, 1, 0, 0), **opts)
     per = max(1, m.sim_steps // calls)
     uniform = not json.load(open(config_path(name))).get("randomize_astro", {}).get("enabled", False)

@@ -148,7 +148,9 @@ typedef struct asg_state {
 /* Engine options.  Zero-initialised fields take the defaults. */
 typedef struct asg_engine_opts {
     int32_t device;         /* CUDA device ordinal (default 0)                    */
-    int32_t chunk_steps;    /* steps per captured CUDA graph (default 32)          */
+    int32_t chunk_steps;    /* steps per captured CUDA graph (default: asg_create
+                               ~2^23 / neurons as a power of two in [32, 512];
+                               batches and servers 32 and 64)                  */
     int32_t block;          /* threads per block of the step kernel (default 128)  */
     int32_t use_graphs;     /* 0/1 = a CUDA graph of per-step launches (default),
                                -1 = plain launches, 2 = persistent: one cooperative
