@@ -174,6 +174,7 @@ SIGNATURES = {
     "asg_astro_create": (C.c_int, [C.c_uint32, c_double_p, c_double_p, c_double_p, c_double_p,
                                    c_double_p, c_double_p, c_double_p, vpp]),
     "asg_astro_destroy": (C.c_int, [vp, c_double_p, c_double_p, c_double_p]),
+    "asg_astro_set_shape": (C.c_int, [vp, C.c_int32]),
     "asg_astro_push_input": (C.c_int, [vp, c_double_p]),
     "asg_astro_pull_calcium": (C.c_int, [vp, c_double_p]),
     "asg_astro_update": (C.c_int, [vp, c_double_p, C.c_double, C.c_int32, C.c_double, C.c_int32,

@@ -118,6 +118,10 @@ class AstroBackend:
         _lib.call("asg_astro_last_timing", self._h, C.byref(ms), C.byref(k))
         return ms.value, k.value
 
+    def set_shape(self, shape: int):
+        """Use launch shape `shape` (raises AsgError outside the valid range)."""
+        _lib.call("asg_astro_set_shape", self._h, int(shape))
+
     def autotune(self, w: ScalingWorkload, steps=20):
         """Pick the fastest launch shape on a scratch copy (state unchanged)."""
         chosen = C.c_int32()

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -54,9 +55,12 @@ struct StepArgs {
     int independent;
     double shared_noise;
     std::uint64_t noise_seed, noise_index;
-    // Bernoulli input (scaling path)
+    // Bernoulli input (scaling path): an event when the draw's 53-bit integer
+    // k satisfies k < p_threshold = ceil(p * 2^53), which is exactly
+    // k * 2^-53 < p (the reference's rng_uniform(...) < p) in integers.
     std::uint64_t seed;
     double p, weight;
+    std::uint64_t p_threshold;
     const std::int64_t* step_base;  // device counter: step = *step_base + step_offset
     int step_offset;
     std::int64_t i0;  // global index of the first cell of this launch (RNG streams)
@@ -68,8 +72,8 @@ __device__ __forceinline__ void advance_cell(const StepArgs& a, const AstroArray
                                              double& ip3, double& hh) {
     double in;
     if (kInput == kInputBernoulli) {
-        in = uniform_at(a.seed, static_cast<std::uint64_t>(a.i0 + i),
-                        1000ULL + static_cast<std::uint64_t>(step)) < a.p
+        in = (mix64(a.seed, static_cast<std::uint64_t>(a.i0 + i),
+                    1000ULL + static_cast<std::uint64_t>(step)) >> 11) < a.p_threshold
                  ? a.weight
                  : 0.0;
     } else {
@@ -99,7 +103,44 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) astro_step_kernel(StepArgs
     const std::int64_t step =
         (kInput == kInputBernoulli) ? (*a.step_base + a.step_offset) : 0;
     const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
-    if (kCells == 2) {
+    if (kCells == 4) {
+        // Four adjacent cells per thread (two 128-bit accesses per array):
+        // four independent RK4 chains to interleave.
+        const std::int64_t quads = a.n / 4;
+        double2* Ca2 = reinterpret_cast<double2*>(s.Ca);
+        double2* IP32 = reinterpret_cast<double2*>(s.IP3);
+        double2* h2 = reinterpret_cast<double2*>(s.h);
+        for (std::int64_t q = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+             q < quads; q += stride) {
+            double2 ca0 = Ca2[2 * q], ip30 = IP32[2 * q], hh0 = h2[2 * q];
+            double2 ca1 = Ca2[2 * q + 1], ip31 = IP32[2 * q + 1], hh1 = h2[2 * q + 1];
+            const std::int64_t i = 4 * q;
+            advance_cell<kUniform, kInput, kNoise>(a, s, i, step, ca0.x, ip30.x, hh0.x);
+            advance_cell<kUniform, kInput, kNoise>(a, s, i + 1, step, ca0.y, ip30.y, hh0.y);
+            advance_cell<kUniform, kInput, kNoise>(a, s, i + 2, step, ca1.x, ip31.x, hh1.x);
+            advance_cell<kUniform, kInput, kNoise>(a, s, i + 3, step, ca1.y, ip31.y, hh1.y);
+            Ca2[2 * q] = ca0;
+            IP32[2 * q] = ip30;
+            h2[2 * q] = hh0;
+            Ca2[2 * q + 1] = ca1;
+            IP32[2 * q + 1] = ip31;
+            h2[2 * q + 1] = hh1;
+            if (kInput == kInputArray) {
+                reinterpret_cast<double2*>(s.input)[2 * q] = make_double2(0.0, 0.0);
+                reinterpret_cast<double2*>(s.input)[2 * q + 1] = make_double2(0.0, 0.0);
+            }
+        }
+        // Up to three tail cells.
+        if (blockIdx.x == 0 && threadIdx.x < static_cast<unsigned>(a.n & 3)) {
+            const std::int64_t i = 4 * quads + threadIdx.x;
+            double ca = s.Ca[i], ip3 = s.IP3[i], hh = s.h[i];
+            advance_cell<kUniform, kInput, kNoise>(a, s, i, step, ca, ip3, hh);
+            s.Ca[i] = ca;
+            s.IP3[i] = ip3;
+            s.h[i] = hh;
+            if (kInput == kInputArray) s.input[i] = 0.0;
+        }
+    } else if (kCells == 2) {
         const std::int64_t pairs = a.n / 2;
         double2* Ca2 = reinterpret_cast<double2*>(s.Ca);
         double2* IP32 = reinterpret_cast<double2*>(s.IP3);
@@ -144,14 +185,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) astro_step_kernel(StepArgs
 struct Shape {
     int cells, block, min_blocks;
 };
-constexpr Shape kShapes[] = {{2, 128, 4}, {1, 128, 8}, {1, 256, 4}, {2, 128, 6},
-                             {1, 128, 6}, {1, 64, 12}};
+constexpr Shape kShapes[] = {{2, 128, 4}, {1, 128, 8}, {1, 256, 4}, {2, 128, 6}, {1, 128, 6},
+                             {1, 64, 12}, {4, 64, 8}, {4, 128, 4}, {2, 128, 5}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 template <bool kUniform, int kInput, bool kNoise>
 cudaError_t launch_astro(int shape, int sms, StepArgs a, AstroArrays s, cudaStream_t st) {
     const Shape sh = kShapes[shape];
-    const std::int64_t units = sh.cells == 2 ? std::max<std::int64_t>(1, a.n / 2) : a.n;
+    const std::int64_t units = std::max<std::int64_t>(1, a.n / sh.cells);
     const std::int64_t want = (units + sh.block - 1) / sh.block;
     const std::int64_t cap = static_cast<std::int64_t>(sms) * sh.min_blocks * 4;
     const int grid = static_cast<int>(std::max<std::int64_t>(1, std::min(want, cap)));
@@ -161,12 +202,24 @@ cudaError_t launch_astro(int shape, int sms, StepArgs a, AstroArrays s, cudaStre
         case 2: astro_step_kernel<kUniform, kInput, kNoise, 1, 256, 4><<<grid, 256, 0, st>>>(a, s); break;
         case 3: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 6><<<grid, 128, 0, st>>>(a, s); break;
         case 4: astro_step_kernel<kUniform, kInput, kNoise, 1, 128, 6><<<grid, 128, 0, st>>>(a, s); break;
-        default: astro_step_kernel<kUniform, kInput, kNoise, 1, 64, 12><<<grid, 64, 0, st>>>(a, s); break;
+        case 5: astro_step_kernel<kUniform, kInput, kNoise, 1, 64, 12><<<grid, 64, 0, st>>>(a, s); break;
+        case 6: astro_step_kernel<kUniform, kInput, kNoise, 4, 64, 8><<<grid, 64, 0, st>>>(a, s); break;
+        case 7: astro_step_kernel<kUniform, kInput, kNoise, 4, 128, 4><<<grid, 128, 0, st>>>(a, s); break;
+        default: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 5><<<grid, 128, 0, st>>>(a, s); break;
     }
     return cudaGetLastError();
 }
 
 __global__ void advance_counter_kernel(std::int64_t* base, std::int64_t by) { *base += by; }
+
+// ceil(p * 2^53): k * 2^-53 < p exactly when the integer k is below it
+// (p * 2^53 is exact, and an integer is below a real number exactly when it
+// is below its ceiling).  p <= 0 or NaN gives no events, p >= 1 every one.
+std::uint64_t bernoulli_threshold(double p) {
+    if (!(p > 0.0)) return 0;
+    if (p >= 1.0) return 1ull << 53;
+    return static_cast<std::uint64_t>(std::ceil(std::ldexp(p, 53)));
+}
 
 AstroK make_astro_k(const double* c, double h_step, int substeps) {
     // c: Kd_IP3_1, Kd_IP3_2, Kd_act, Kd_inh, Km_SERCA, k_IP3R, rate_IP3R,
@@ -466,6 +519,7 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
     a.u = asg::UniformParams{Ca_tot, IP3_0, tau_IP3, delta_IP3, 1.0 / tau_IP3};
     a.seed = seed;
     a.p = p;
+    a.p_threshold = asg::bernoulli_threshold(p);
     a.weight = weight;
     a.step_base = e->step_base.as<std::int64_t>();
 
@@ -540,6 +594,16 @@ int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels) {
 
 }  // extern "C"
 
+extern "C" int asg_astro_set_shape(asg_astro* s, int32_t shape) {
+    asg::clear_error();
+    if (s == nullptr) return asg::fail(ASG_ERR_ARG, "asg_astro_set_shape: NULL handle");
+    if (shape < 0 || shape >= asg::kNumShapes)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_set_shape: shape %d not in [0, %d)", shape,
+                         asg::kNumShapes);
+    reinterpret_cast<AstroEngine*>(s)->shape = shape;
+    return ASG_OK;
+}
+
 extern "C" int asg_astro_autotune(asg_astro* s, const double* consts, double h_step,
                                   int32_t substeps, int32_t steps, int32_t* chosen,
                                   double* us_per_step) {
@@ -570,6 +634,7 @@ extern "C" int asg_astro_autotune(asg_astro* s, const double* consts, double h_s
                              0.04911592657233997, 1.0 / 1058.7589568400845};
     a.seed = 1;
     a.p = 0.01;
+    a.p_threshold = asg::bernoulli_threshold(a.p);
     a.weight = 0.2;
     a.step_base = e->step_base.as<std::int64_t>();
     int best = e->shape;

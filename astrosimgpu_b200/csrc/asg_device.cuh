@@ -207,9 +207,11 @@ __device__ __forceinline__ void astro_rk4(const AstroK& k, double ca_tot, double
                 sIP3 = r.IP3;
                 sh = r.h;
             } else if (st < 3) {
-                sCa = sCa + 2.0 * r.Ca;
-                sIP3 = sIP3 + 2.0 * r.IP3;
-                sh = sh + 2.0 * r.h;
+                // s + 2r in one rounding: 2r is exact, so fma(2, r, s) is
+                // the same IEEE result as s + (2.0 * r) (while 2r is finite)
+                sCa = fma(2.0, r.Ca, sCa);
+                sIP3 = fma(2.0, r.IP3, sIP3);
+                sh = fma(2.0, r.h, sh);
             } else {
                 sCa = sCa + r.Ca;
                 sIP3 = sIP3 + r.IP3;

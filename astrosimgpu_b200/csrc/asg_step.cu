@@ -600,8 +600,8 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
                         sV = r.V;
                         sw = r.w;
                     } else if (stg < 3) {
-                        sV = sV + 2.0 * r.V;
-                        sw = sw + 2.0 * r.w;
+                        sV = fma(2.0, r.V, sV);  // = sV + 2.0 * r.V: 2r is exact
+                        sw = fma(2.0, r.w, sw);
                     } else {
                         sV = sV + r.V;
                         sw = sw + r.w;

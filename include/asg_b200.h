@@ -298,6 +298,10 @@ int asg_astro_pull_state(asg_astro* s, double* Ca, double* IP3, double* h);
  * its index and per-step microseconds (may be NULL). */
 int asg_astro_autotune(asg_astro* s, const double* consts, double h_step, int32_t substeps,
                        int32_t steps, int32_t* chosen, double* us_per_step);
+/* Use launch shape `shape` (an index asg_astro_autotune may return) for this
+ * handle; ASG_ERR_ARG names the valid range.  Every shape gives the same
+ * bits.  No counterpart in the reference (a tuning knob, like autotune). */
+int asg_astro_set_shape(asg_astro* s, int32_t shape);
 /* Device ms of the last run call and kernels launched. */
 int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels);
 
