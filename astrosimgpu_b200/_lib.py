@@ -107,7 +107,7 @@ class State(C.Structure):
 class EngineOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("chunk_steps", C.c_int32), ("block", C.c_int32),
                 ("use_graphs", C.c_int32), ("sic_mode", C.c_int32), ("pdl", C.c_int32),
-                ("push_mode", C.c_int32), ("mem_budget", C.c_uint64)]
+                ("push_mode", C.c_int32), ("mem_budget", C.c_uint64), ("occupancy", C.c_int32)]
 
 
 class ServeOpts(C.Structure):

@@ -22,6 +22,7 @@ EngineConfig config_from(const asg_engine_opts* o) {
         c.pdl = o->pdl >= 0;
         c.push_mode = o->push_mode;
         c.mem_budget = o->mem_budget;
+        c.occupancy = o->occupancy;
     }
     return c;
 }
@@ -193,6 +194,7 @@ int autotune_engine(Engine& e, int32_t steps, asg_engine_opts* chosen) {
         chosen->pdl = e.cfg.pdl ? 0 : -1;
         chosen->push_mode = e.cfg.push_mode;
         chosen->mem_budget = e.cfg.mem_budget;
+        chosen->occupancy = e.cfg.occupancy;
     }
     (void)block0;
     (void)mode0;

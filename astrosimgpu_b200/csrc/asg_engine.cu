@@ -767,6 +767,14 @@ int Engine::rebuild() {
                                  side_work.size() * sizeof(Work), cudaMemcpyHostToDevice, stream));
     ASG_CUDA(cudaMemsetAsync(d_stats.get(), 0, cap_insts * 8 * sizeof(unsigned long long), stream));
     ASG_CUDA(cudaStreamSynchronize(stream));
+    // Step kernel form: a step of more than two waves of the latency form
+    // (4 blocks of 128 threads per SM) is throughput-bound, and the
+    // high-occupancy form (6 blocks per SM, some spilled registers) runs it
+    // faster; a smaller step is bound by its dependent round trips, which
+    // the latency form keeps fewest.
+    wide = cfg.block == 128 &&
+           (cfg.occupancy == 2 ||
+            (cfg.occupancy == 0 && work.size() > static_cast<std::size_t>(2 * 4 * sms)));
     persistent_grid = 0;
     if (cfg.use_graphs == 2 && !work.empty()) {
         const int cap = persistent_blocks(B);
@@ -854,7 +862,7 @@ cudaError_t Engine::issue_steps(int steps) {
             e = cudaStreamWaitEvent(stream, ev_side_done[((k - side_lead) / G) % kSideEvents], 0);
         if (e == cudaSuccess)
             e = launch_step(d_insts.as<InstDev>(), d_work.as<Work>(), static_cast<int>(work.size()),
-                            cfg.block, k, cfg.pdl && k > 0, stream);
+                            cfg.block, k, cfg.pdl && k > 0, wide, stream);
     }
     if (side_on && e == cudaSuccess) {
         e = cudaEventRecord(ev_side_join, side);

@@ -203,7 +203,8 @@ cudaError_t launch_sic_batch(const InstDev* insts, const Work* work, int n_work,
 // One step launch; with `pdl` the launch may start while the previous kernel
 // of the stream is still running (the kernel waits for it before any access
 // to instance state).
+// `wide`: the high-occupancy form (block 128 only; same arithmetic).
 cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
-                        bool pdl, cudaStream_t stream);
+                        bool pdl, bool wide, cudaStream_t stream);
 
 }  // namespace asg

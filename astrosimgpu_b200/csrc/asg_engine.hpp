@@ -60,6 +60,7 @@ struct EngineConfig {
     bool pdl = true;   // programmatic dependent launch between steps
     int push_mode = 0; // 0 deferred push when delays allow, 1 always in the spiking block
     std::uint64_t mem_budget = 0;
+    int occupancy = 0;  // 0 auto, 1 latency form, 2 high-occupancy form of the step kernel
 };
 
 class Engine {
@@ -134,6 +135,7 @@ private:
     static constexpr std::size_t kMaxGraphs = 4;
     std::vector<std::pair<int, cudaGraphExec_t>> graphs;
     bool graph_mode() const { return cfg.use_graphs == 0 || cfg.use_graphs == 1; }
+    bool wide = false;  // launches use the high-occupancy form of the step kernel
     cudaGraphExec_t find_graph(int steps);
     int capture_graph(int steps);
     void drop_graphs();

@@ -942,8 +942,9 @@ __device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, co
     help_push(I, S, wk);
 }
 
-__global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restrict__ insts,
-                                                         const Work* __restrict__ work, int k) {
+// One step of every resident instance (the body of both kernel forms below).
+__device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
+                                          const Work* __restrict__ work, int k) {
     // Stage this block's instance descriptor and step arithmetic in shared
     // memory.  Both depend only on data written before the chunk started, so
     // this overlaps the tail of the previous step's grid.
@@ -967,6 +968,23 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restri
     // predecessor to complete before touching state it writes.
     asm volatile("griddepcontrol.launch_dependents;");
     run_role<true>(I, s_info, wk);
+}
+
+// Two forms of the step kernel, same arithmetic: step_kernel allows blocks of
+// up to kMaxBlock threads and 128 registers per thread (4 blocks of 128
+// threads per SM; the fewest dependent round trips, for steps of a few
+// waves); step_kernel_wide is for 128-thread blocks at 6 per SM (80
+// registers, some spilled: more warps to hide latency when a step is many
+// waves of blocks).
+__global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restrict__ insts,
+                                                         const Work* __restrict__ work, int k) {
+    step_body(insts, work, k);
+}
+
+__global__ void __launch_bounds__(128, 6) step_kernel_wide(const InstDev* __restrict__ insts,
+                                                           const Work* __restrict__ work,
+                                                           int k) {
+    step_body(insts, work, k);
 }
 
 // Grid-wide barrier of the persistent chunk kernel (all blocks co-resident
@@ -1171,7 +1189,7 @@ cudaError_t launch_chunk_persistent(const InstDev* insts, const Work* work, int 
 }
 
 cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
-                        bool pdl, cudaStream_t stream) {
+                        bool pdl, bool wide, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(static_cast<unsigned>(n_work));
     cfg.blockDim = dim3(static_cast<unsigned>(block));
@@ -1182,6 +1200,7 @@ cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int 
     attr[0].val.programmaticStreamSerializationAllowed = pdl ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (wide && block == 128) return cudaLaunchKernelEx(&cfg, step_kernel_wide, insts, work, k);
     return cudaLaunchKernelEx(&cfg, step_kernel, insts, work, k);
 }
 

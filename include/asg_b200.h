@@ -161,6 +161,11 @@ typedef struct asg_engine_opts {
                                push blocks when both spike delays are >= 2 steps
                                (default), 1 = pushed by the spiking block      */
     uint64_t mem_budget;    /* device bytes the engine may hold (0 = 90% free)     */
+    int32_t occupancy;      /* step kernel form: 0 auto (by the number of blocks
+                               a step launches), 1 latency form (fewest round
+                               trips, 128 registers), 2 high-occupancy form
+                               (6 blocks of 128 threads per SM; block 128 only).
+                               Both forms give the same bits.                  */
 } asg_engine_opts;
 
 /* ------------------------------------------------------ single network

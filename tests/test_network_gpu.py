@@ -194,11 +194,12 @@ def test_sic_forms_bitwise():
 def test_burst_push_paths_bitwise():
     """The initial burst of the paper-sparse network (up to ~400 spikes in a
     step, tens of arrivals per target and slot): the deferred push with every
-    block helping, the in-block push and the persistent kernel give the same
-    bits, and the short-list overflow path is taken."""
+    block helping, the in-block push, the persistent kernel and the
+    high-occupancy form of the step kernel give the same bits, and the
+    short-list overflow path is taken."""
     m = Model(config_path("paper_sparse_dt005"), pre_time=0.0)
     outs = []
-    for opts in (dict(), dict(push_mode=1), dict(use_graphs=2, block=256)):
+    for opts in (dict(), dict(push_mode=1), dict(use_graphs=2, block=256), dict(occupancy=2)):
         n = Network(m, record=rec_all(), **opts)
         n.step(800)
         outs.append((n.fetch_spikes(), n.state(), n.counters(), opts, n.current_step,
@@ -210,6 +211,29 @@ def test_burst_push_paths_bitwise():
             len(sp[0]), c, opts, cur, tim, float(np.nanmean(st["V"])))
         for k in STATE_KEYS:
             assert np.array_equal(st[k], st0[k]), k
+
+
+def test_burst_overflow_both_merge_paths_parity():
+    """A synchronous burst at high in-degree against the oracle: excitatory
+    targets of more than 1024 in-edges (more than 32 bitmap words: merge by
+    summary) and inhibitory targets of a few hundred (all words in one batch)
+    both receive tens of arrivals in one slot; spikes must be identical and
+    the state within the network tolerance."""
+    cfg = json.load(open(config_path("paper_sparse_dt005")))
+    cfg["N"].update({"N_E": 2400, "N_I": 600, "N_A": 3000})
+    cfg["connectivity"]["p_primary"] = 0.5
+    text = json.dumps(cfg)
+    m = Model(text=text, pre_time=0.0)
+    deg_e = np.bincount(m.table(0)[1]).max()
+    deg_i = np.bincount(m.table(1)[1]).max()
+    assert deg_e > 1024 and deg_i <= 1024, (deg_e, deg_i)
+    g, r, gsp, rsp = run_pair(text=text, steps=800, chunks=2)
+    assert_same_spikes(gsp, rsp)
+    assert_state_close(g, r)
+    per_step = np.bincount(gsp[0])
+    # ~200 coincident spikes (a fifth of them inhibitory) at p = 0.5: tens of
+    # arrivals per target and slot in every ring
+    assert per_step.max() > 150, per_step.max()
 
 
 def test_sic_modes_and_block_sizes_bitwise():
