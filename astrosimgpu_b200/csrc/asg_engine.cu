@@ -396,8 +396,19 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     D.d_a2n = d.d_a2n_steps;
     D.slots = std::max({1, D.d_e, D.d_i, D.d_a2n}) + 1;
     D.sic_interval = d.sic_interval;
+    static const std::uint32_t zero_rs[1] = {0};
+    auto rs_of = [](const asg_csr& c) { return c.n_sources ? c.row_start : zero_rs; };
+    // SIC form.  A one-step delay needs the fused form.  In auto mode a
+    // large network (N >= 2^16: its neuron and astrocyte blocks alone fill
+    // the GPU more than twice, so the step is throughput-bound) with short
+    // SIC lists also sums each target's SIC in its neuron thread, which
+    // saves the SIC role's blocks (a third of the step's); a smaller network
+    // keeps the SIC role, which runs beside the neuron role (lower latency).
+    const std::uint32_t sic_mx =
+        NA > 0 ? sic_max_edges(NA, rs_of(d.astro_neuron), d.astro_neuron.target, N) : 0;
+    const bool fuse_auto = D.d_a2n < 2 || (N >= (1u << 16) && sic_mx <= kSicEdgesPerPart);
     D.fused_sic = cfg.sic_mode == 1 ? 1 : cfg.sic_mode == 2 ? (D.d_a2n >= 2 ? 0 : 1)
-                                                            : (D.d_a2n >= 2 ? 0 : 1);
+                                                            : (fuse_auto ? 1 : 0);
     D.stp_on = d.stp.enabled != 0;
     // Deferred push needs both spike delays >= 2 steps (the push of step s
     // runs in step s+1 and must land before step s+d reads it).
@@ -459,8 +470,6 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     D.inv_tau_u = 1.0 / uval[2];
 
     // Host preprocessing of the tables.
-    static const std::uint32_t zero_rs[1] = {0};
-    auto rs_of = [](const asg_csr& c) { return c.n_sources ? c.row_start : zero_rs; };
     InRingHost rex = make_in_ring(NE, rs_of(d.exc_primary), d.exc_primary.target, N);
     InRingHost rin = make_in_ring(NI, rs_of(d.inh_primary), d.inh_primary.target, N);
     InRingHost ras = make_in_ring(NE, rs_of(d.neuron_astro), d.neuron_astro.target, NA);
@@ -477,8 +486,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     D.sic_lead = D.sic_side ? std::min(D.d_a2n - kSicBatchSteps, kSicRing - kSicBatchSteps - 8) : 0;
     D.sic_ring = D.sic_side ? kSicRing : 2;
     if (!D.fused_sic && !D.sic_side) {
-        const std::uint32_t mx = sic_max_edges(NA, rs_of(d.astro_neuron), d.astro_neuron.target, N);
-        const int want = static_cast<int>((mx + kSicEdgesPerPart - 1) / kSicEdgesPerPart);
+        const int want = static_cast<int>((sic_mx + kSicEdgesPerPart - 1) / kSicEdgesPerPart);
         D.sic_parts = std::max(1, std::min({want, kMaxSicParts, D.d_a2n - 1}));
     }
     SicHost sic = make_sic(NA, rs_of(d.astro_neuron), d.astro_neuron.target, N,

@@ -236,6 +236,30 @@ def test_burst_overflow_both_merge_paths_parity():
     assert per_step.max() > 150, per_step.max()
 
 
+def test_large_network_sic_forms_bitwise():
+    """A network of 2^16+ neurons with short SIC lists (the serving shape,
+    astrocytes active from the start): the automatic form (SIC summed in the
+    neuron thread, high-occupancy step kernel), the SIC role and the latency
+    form of the step kernel give the same bits."""
+    from astrosimgpu_b200.workloads import serving_config
+    cfg = json.loads(serving_config(70000, 5, 10.0))
+    cfg["astrocyte"]["Ca_init"] = 0.35
+    cfg["astrocyte"]["IP3"] = 0.6
+    m = Model(text=json.dumps(cfg), pre_time=0.0, fixed_indegree=100, gen_device=0)
+    outs = []
+    for opts in (dict(), dict(sic_mode=2), dict(sic_mode=1, occupancy=1)):
+        n = Network(m, record=rec_all(), **opts)
+        n.step(60)
+        outs.append((n.fetch_spikes(), n.state(), n.counters()))
+        del n
+    (sp0, st0, c0) = outs[0]
+    assert c0["sic_edges"] > 0 and c0["spikes"] > 0, c0
+    for sp, st, c in outs[1:]:
+        assert np.array_equal(sp[0], sp0[0]) and np.array_equal(sp[1], sp0[1])
+        for k in STATE_KEYS:
+            assert np.array_equal(st[k], st0[k]), k
+
+
 def test_sic_modes_and_block_sizes_bitwise():
     """The separate SIC role and the fused form, any block size, per-step
     graph launches, plain launches and the persistent chunk kernel give
