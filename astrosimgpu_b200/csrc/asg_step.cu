@@ -515,6 +515,10 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
         const std::size_t ts_in = static_cast<std::size_t>(slot) * I.ring_in.n_targets + c;
         const std::uint32_t n_ex = __ldcg(I.ring_ex.cnt + ts_ex);
         const std::uint32_t n_in = __ldcg(I.ring_in.cnt + ts_in);
+        // The first excitatory list value, loaded before the count is known:
+        // with a single arrival (the common case) the sum needs no second
+        // round trip.
+        const double v0_ex = __ldcg(I.ring_ex.lval + ts_ex * kListCap);
         const bool sic_due = S.sic_now != 0;
         double Isic = (sic_due && !I.fused_sic)
                           ? __ldcg(I.sic_val +
@@ -547,12 +551,14 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
 
         // apply_arrivals (network.cpp:301-338): both short lists in one batch.
         ShortList lex{}, lin{};
-        if (n_ex) lex = load_list(I.ring_ex, ts_ex);
+        if (n_ex > 1) lex = load_list(I.ring_ex, ts_ex);
         if (n_in) lin = load_list(I.ring_in, ts_in);
         double exc_in = 0.0, inh_in = 0.0;
         if (n_ex) {
             I.ring_ex.cnt[ts_ex] = 0;
-            const double ex = sum_arrivals<false>(I.ring_ex, slot, c, n_ex, lex);
+            // one arrival: 0.0 + v, the sum sum_arrivals forms for n = 1
+            const double ex = n_ex == 1 ? 0.0 + v0_ex
+                                        : sum_arrivals<false>(I.ring_ex, slot, c, n_ex, lex);
             if (ex != 0.0) add_syn(ex, exc_in, inh_in);
         }
         if (n_in) {
