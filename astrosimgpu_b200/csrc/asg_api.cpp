@@ -347,7 +347,14 @@ int asg_batch_create(int32_t n, const asg_network_desc* const* descs, const asg_
         return asg::fail(ASG_ERR_ARG, "asg_batch_create: bad arguments");
     *out = nullptr;
     auto h = std::make_unique<BatchHandle>();
-    h->eng = std::make_unique<Engine>(asg::config_from(opts));
+    asg::EngineConfig cfg = asg::config_from(opts);
+    // A batch of 2^16+ neurons in all runs throughput-bound steps: its
+    // instances with short SIC lists sum SIC in their neuron threads.
+    std::uint64_t total = 0;
+    for (int32_t i = 0; i < n; ++i)
+        if (descs[i] != nullptr) total += static_cast<std::uint64_t>(descs[i]->n_exc) + descs[i]->n_inh;
+    cfg.large_total = total >= (1u << 16);
+    h->eng = std::make_unique<Engine>(cfg);
     ASG_TRY(h->eng->init());
     for (int32_t i = 0; i < n; ++i) {
         if (descs[i] == nullptr) return asg::fail(ASG_ERR_ARG, "asg_batch_create: descs[%d] NULL", i);

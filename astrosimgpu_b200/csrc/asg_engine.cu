@@ -399,14 +399,16 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     static const std::uint32_t zero_rs[1] = {0};
     auto rs_of = [](const asg_csr& c) { return c.n_sources ? c.row_start : zero_rs; };
     // SIC form.  A one-step delay needs the fused form.  In auto mode a
-    // large network (N >= 2^16: its neuron and astrocyte blocks alone fill
-    // the GPU more than twice, so the step is throughput-bound) with short
-    // SIC lists also sums each target's SIC in its neuron thread, which
-    // saves the SIC role's blocks (a third of the step's); a smaller network
-    // keeps the SIC role, which runs beside the neuron role (lower latency).
+    // large network (N >= 2^16, or an instance of a batch of 2^16+ neurons
+    // in all: the step's blocks fill the GPU more than twice, so it is
+    // throughput-bound) with short SIC lists also sums each target's SIC in
+    // its neuron thread, which saves the SIC role's blocks (a third of the
+    // step's); a smaller network keeps the SIC role, which runs beside the
+    // neuron role (lower latency).
     const std::uint32_t sic_mx =
         NA > 0 ? sic_max_edges(NA, rs_of(d.astro_neuron), d.astro_neuron.target, N) : 0;
-    const bool fuse_auto = D.d_a2n < 2 || (N >= (1u << 16) && sic_mx <= kSicEdgesPerPart);
+    const bool fuse_auto =
+        D.d_a2n < 2 || ((N >= (1u << 16) || cfg.large_total) && sic_mx <= kSicEdgesPerPart);
     D.fused_sic = cfg.sic_mode == 1 ? 1 : cfg.sic_mode == 2 ? (D.d_a2n >= 2 ? 0 : 1)
                                                             : (fuse_auto ? 1 : 0);
     D.stp_on = d.stp.enabled != 0;

@@ -61,6 +61,7 @@ struct EngineConfig {
     int push_mode = 0; // 0 deferred push when delays allow, 1 always in the spiking block
     std::uint64_t mem_budget = 0;
     int occupancy = 0;  // 0 auto, 1 latency form, 2 high-occupancy form of the step kernel
+    bool large_total = false;  // the engine will hold 2^16+ neurons in all (auto SIC form)
 };
 
 class Engine {

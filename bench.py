@@ -182,7 +182,7 @@ def bench_astro_scaling(args, rank, world, pg):
     w = ScalingWorkload(n, seed=1 + rank)
     Ca, IP3, h = w.initial_state()
     eng = AstroBackend(Ca, IP3, h)
-    shape, tuned_us = eng.autotune(w, steps=10)
+    shape, tuned_us = eng.autotune(w, steps=30)  # 9 shapes x 2 passes x 30 steps, ~0.13 s
     # warm-up (untimed)
     step = 0
     for _ in range(args.warmup):

@@ -156,10 +156,11 @@ typedef struct asg_engine_opts {
                                -1 = plain launches, 2 = persistent: one cooperative
                                launch per chunk, bounded grid barrier per step    */
     int32_t sic_mode;       /* 0 auto, 1 fused into the neuron role, 2 own role.
-                               Auto fuses for a one-step SIC delay and for a
-                               network of >= 2^16 neurons with <= 160 SIC edges
-                               per target; otherwise side-stream batches when the
-                               delay is >= 12 steps, else the own role.        */
+                               Auto fuses for a one-step SIC delay and, with
+                               <= 160 SIC edges per target, for a network (or a
+                               batch) of >= 2^16 neurons; otherwise side-stream
+                               batches when the delay is >= 12 steps, else the
+                               own role.                                        */
     int32_t pdl;            /* 0 = programmatic dependent launch (default), -1 off */
     int32_t push_mode;      /* 0 = spikes pushed one step later by load-balanced
                                push blocks when both spike delays are >= 2 steps

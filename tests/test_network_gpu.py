@@ -300,6 +300,31 @@ def test_batch_equals_single_bitwise(mode):
             assert np.array_equal(a[k], c[k]), (i, k)
 
 
+def test_large_batch_fused_sic_equals_single_bitwise():
+    """A batch of 2^16 neurons in all sums SIC in the neuron threads (its
+    instances are small, so alone each runs the SIC role): the same bits."""
+    cfg = json.load(open(config_path("use_case")))
+    cfg["N"].update({"N_E": 6554, "N_I": 1638, "N_A": 1638})
+    cfg["connectivity"]["p_primary"] = 0.02
+    cfg["astrocyte"]["Ca_init"] = 0.35
+    cfg["astrocyte"]["IP3"] = 0.6
+    text = json.dumps(cfg)
+    models = [Model(text=text, seed=s, pre_time=0.0) for s in range(1, 9)]
+    assert sum(m.desc().n_exc + m.desc().n_inh for m in models) >= 1 << 16
+    b = Batch(models, record=rec_all())
+    b.step(150)
+    assert b.counters(0)["sic_edges"] > 0
+    for i in (0, 5):
+        n = Network(models[i], record=rec_all())
+        n.step(150)
+        s1, s2 = n.fetch_spikes(), b.fetch_spikes(i)
+        assert np.array_equal(s1[0], s2[0]) and np.array_equal(s1[1], s2[1])
+        a, c = n.state(), b.state(i)
+        for k in STATE_KEYS:
+            assert np.array_equal(a[k], c[k]), (i, k)
+        n.close()
+
+
 def test_checkpoint_restore_bitwise():
     m = Model(config_path("use_case"), pre_time=0.0)
     n = Network(m, record=rec_all())
