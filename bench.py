@@ -346,7 +346,7 @@ def bench_batched(sim_ms=500.0, n_inst=64, autotune=True):
         plain_kernels += k
         net.close()
     b = Batch(models, record=rec, chunk_steps=128)
-    tuned = b.autotune(256) if autotune else None
+    tuned = b.autotune(1024) if autotune else None  # long enough to rank chunk lengths
     b.step(64)
     b.step(steps)
     bms, bk = b.last_timing()
