@@ -4,6 +4,8 @@
 
 #include "asg_engine.hpp"
 
+#include <omp.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -81,31 +83,65 @@ struct InRingHost {
     std::uint32_t words = 0;
 };
 
+//
+// A stable counting sort by target, on the host's cores: thread k takes the
+// sources of a contiguous range (about m / T edges) and counts its edges per
+// target; per target, an exclusive prefix over the threads gives each
+// thread the number of that target's in-edges from earlier sources; each
+// thread then numbers its edges in (source, row position) order from there.
+// Every edge gets the number the one-thread pass would give it.
 InRingHost make_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std::uint32_t* tg,
                         std::uint32_t n_targets) {
     InRingHost r;
     const std::uint32_t m = rs[n_src];
-    std::vector<std::uint32_t> deg(n_targets, 0);
-    for (std::uint32_t e = 0; e < m; ++e) deg[tg[e]]++;
+    const std::size_t n = std::max<std::uint32_t>(n_targets, 1);
+    // threads: one per 2^16 edges at most, and per-thread counters within 256 MB
+    int T = std::min<int>(omp_get_max_threads(), static_cast<int>(m >> 16));
+    T = std::max(1, std::min<int>(T, static_cast<int>((std::size_t{1} << 26) / n)));
+    std::vector<std::uint32_t> cut(static_cast<std::size_t>(T) + 1, n_src);
+    cut[0] = 0;
+    for (int k = 1; k < T; ++k) {  // first source whose row starts at or after k*m/T
+        const std::uint64_t e0 = static_cast<std::uint64_t>(m) * k / T;
+        cut[k] = static_cast<std::uint32_t>(std::lower_bound(rs, rs + n_src, e0) - rs);
+    }
+    std::vector<std::uint32_t> cnt(static_cast<std::size_t>(T) * n, 0);
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int k = 0; k < T; ++k) {
+        std::uint32_t* h = cnt.data() + static_cast<std::size_t>(k) * n;
+        for (std::uint32_t e = rs[cut[k]]; e < rs[cut[k + 1]]; ++e) h[tg[e]]++;
+    }
     r.wbase.assign(n_targets + 1, 0);
+    std::vector<std::uint32_t> deg(n_targets, 0);
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (std::int64_t t = 0; t < static_cast<std::int64_t>(n_targets); ++t) {
+        std::uint32_t run = 0;
+        for (int k = 0; k < T; ++k) {
+            std::uint32_t& c = cnt[static_cast<std::size_t>(k) * n + static_cast<std::size_t>(t)];
+            const std::uint32_t v = c;
+            c = run;
+            run += v;
+        }
+        deg[static_cast<std::size_t>(t)] = run;
+    }
     for (std::uint32_t t = 0; t < n_targets; ++t) r.wbase[t + 1] = r.wbase[t] + (deg[t] + 31) / 32;
     r.words = r.wbase[n_targets];
     r.edge.assign(m, 0);
-    std::vector<std::uint32_t> next(n_targets, 0);
-    // Sources ascending, each row in CSR order: in-edge numbers follow
-    // (source, position in the source's row).
-    for (std::uint32_t s = 0; s < n_src; ++s) {
-        for (std::uint32_t e = rs[s]; e < rs[s + 1]; ++e) {
-            const std::uint32_t t = tg[e];
-            const std::uint32_t p = next[t]++;
-            const std::uint32_t nw = r.wbase[t + 1] - r.wbase[t];
-            const std::uint32_t G = (nw + 63) / 64;
-            const unsigned long long bit = static_cast<unsigned long long>(r.wbase[t]) * 32 + p;
-            // A target of at most 32 words reads all its words at once and
-            // never its summary: its pushes skip the summary update.
-            const unsigned long long dense = nw <= 32 ? 1ull : 0ull;
-            r.edge[e] = bit | (static_cast<unsigned long long>(t) << 32) | (dense << 57) |
-                        (static_cast<unsigned long long>((p / 32) / G) << 58);
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int k = 0; k < T; ++k) {
+        std::uint32_t* next = cnt.data() + static_cast<std::size_t>(k) * n;
+        for (std::uint32_t s = cut[k]; s < cut[k + 1]; ++s) {
+            for (std::uint32_t e = rs[s]; e < rs[s + 1]; ++e) {
+                const std::uint32_t t = tg[e];
+                const std::uint32_t p = next[t]++;
+                const std::uint32_t nw = r.wbase[t + 1] - r.wbase[t];
+                const std::uint32_t G = (nw + 63) / 64;
+                const unsigned long long bit = static_cast<unsigned long long>(r.wbase[t]) * 32 + p;
+                // A target of at most 32 words reads all its words at once and
+                // never its summary: its pushes skip the summary update.
+                const unsigned long long dense = nw <= 32 ? 1ull : 0ull;
+                r.edge[e] = bit | (static_cast<unsigned long long>(t) << 32) | (dense << 57) |
+                            (static_cast<unsigned long long>((p / 32) / G) << 58);
+            }
         }
     }
     return r;
@@ -190,6 +226,18 @@ SicHost make_sic(std::uint32_t NA, const std::uint32_t* rs, const std::uint32_t*
     return s;
 }
 
+// The first index e in [0, m) with bad(e), or m; large ranges are scanned
+// on all of the host's cores.
+template <class Bad>
+std::uint32_t first_bad(std::uint32_t m, Bad bad) {
+    std::uint32_t first = m;
+#pragma omp parallel for reduction(min : first) schedule(static) if (m >= (1u << 16))
+    for (std::int64_t e = 0; e < static_cast<std::int64_t>(m); ++e)
+        if (bad(static_cast<std::uint32_t>(e)) && static_cast<std::uint32_t>(e) < first)
+            first = static_cast<std::uint32_t>(e);
+    return first;
+}
+
 int check_csr(const char* name, const asg_csr& c, std::uint32_t n_src, std::uint32_t n_tgt) {
     if (c.n_sources != n_src)
         return fail(ASG_ERR_ARG, "%s: n_sources %u, expected %u", name, c.n_sources, n_src);
@@ -197,15 +245,15 @@ int check_csr(const char* name, const asg_csr& c, std::uint32_t n_src, std::uint
         return fail(ASG_ERR_ARG, "%s: row_start is NULL", name);
     if (n_src == 0) return ASG_OK;
     if (c.row_start[0] != 0) return fail(ASG_ERR_ARG, "%s: row_start[0] != 0", name);
-    for (std::uint32_t s = 0; s < n_src; ++s)
-        if (c.row_start[s + 1] < c.row_start[s])
-            return fail(ASG_ERR_ARG, "%s: row_start decreases at %u", name, s);
+    const std::uint32_t s =
+        first_bad(n_src, [&](std::uint32_t i) { return c.row_start[i + 1] < c.row_start[i]; });
+    if (s < n_src) return fail(ASG_ERR_ARG, "%s: row_start decreases at %u", name, s);
     const std::uint32_t m = c.row_start[n_src];
     if (m > 0 && c.target == nullptr) return fail(ASG_ERR_ARG, "%s: target is NULL", name);
-    for (std::uint32_t e = 0; e < m; ++e)
-        if (c.target[e] >= n_tgt)
-            return fail(ASG_ERR_ARG, "%s: target[%u] = %u out of range (%u)", name, e,
-                        c.target[e], n_tgt);
+    const std::uint32_t e = first_bad(m, [&](std::uint32_t i) { return c.target[i] >= n_tgt; });
+    if (e < m)
+        return fail(ASG_ERR_ARG, "%s: target[%u] = %u out of range (%u)", name, e, c.target[e],
+                    n_tgt);
     return ASG_OK;
 }
 
@@ -213,16 +261,17 @@ int check_uniform(const char* name, const asg_csr& c, std::uint32_t n_src, doubl
                   const asg_stp& stp) {
     if (n_src == 0) return ASG_OK;
     const std::uint32_t m = c.row_start[n_src];
-    for (std::uint32_t e = 0; e < m; ++e) {
-        if (c.weight && c.weight[e] != w)
-            return fail(ASG_ERR_UNSUPPORTED,
-                        "%s: per-edge weight %g differs from the set weight %g (the engine "
-                        "takes one weight per set, as the reference builds them)",
-                        name, c.weight[e], w);
-        if (c.delay_steps && c.delay_steps[e] != d)
-            return fail(ASG_ERR_UNSUPPORTED, "%s: per-edge delay %d differs from the set delay %d",
-                        name, c.delay_steps[e], d);
-    }
+    const std::uint32_t e = first_bad(m, [&](std::uint32_t i) {
+        return (c.weight && c.weight[i] != w) || (c.delay_steps && c.delay_steps[i] != d);
+    });
+    if (e < m && c.weight && c.weight[e] != w)
+        return fail(ASG_ERR_UNSUPPORTED,
+                    "%s: per-edge weight %g differs from the set weight %g (the engine "
+                    "takes one weight per set, as the reference builds them)",
+                    name, c.weight[e], w);
+    if (e < m)
+        return fail(ASG_ERR_UNSUPPORTED, "%s: per-edge delay %d differs from the set delay %d",
+                    name, c.delay_steps[e], d);
     if (stp.enabled && (c.stp_x || c.stp_u || c.stp_t_last)) {
         for (std::uint32_t s = 0; s < n_src; ++s) {
             for (std::uint32_t e = c.row_start[s]; e < c.row_start[s + 1]; ++e) {
