@@ -333,6 +333,7 @@ Engine::~Engine() {
     }
     insts.clear();
     if (side) cudaStreamDestroy(side);
+    if (upload) cudaStreamDestroy(upload);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -355,6 +356,7 @@ int Engine::init() {
     }
     ASG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     ASG_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    ASG_CUDA(cudaStreamCreateWithFlags(&upload, cudaStreamNonBlocking));
     ASG_CUDA(cudaEventCreateWithFlags(&ev_side_fork, cudaEventDisableTiming));
     ASG_CUDA(cudaEventCreateWithFlags(&ev_side_join, cudaEventDisableTiming));
     for (int q = 0; q < kSideEvents; ++q) {
@@ -406,9 +408,10 @@ int Engine::footprint(const asg_network_desc& d, int chunk_steps, std::uint64_t*
 
 int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int64_t first,
                 std::int64_t end, bool keep_spikes, int* id_out) {
-    // Chunks in flight report statistics by instance position: gather them
-    // before the instance list changes.
-    ASG_TRY(finish_pending());
+    // The chunks in flight keep running while the tables are prepared and
+    // uploaded (on the upload stream, into a new arena); they are collected
+    // only before the instance list changes, since they report statistics by
+    // instance position.
     const std::uint32_t NE = d.n_exc, NI = d.n_inh, N = NE + NI, NA = d.n_astro;
     if (d.dt <= 0.0) return fail(ASG_ERR_ARG, "dt must be positive");
     if (d.substeps < 1) return fail(ASG_ERR_ARG, "substeps must be at least 1");
@@ -647,14 +650,14 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
             if (s.bytes > 0) {
                 if (s.src != nullptr) {
                     ASG_CUDA(cudaMemcpyAsync(base + off, s.src, s.bytes, cudaMemcpyHostToDevice,
-                                             stream));
+                                             upload));
                 } else {
-                    ASG_CUDA(cudaMemsetAsync(base + off, 0, s.bytes, stream));
+                    ASG_CUDA(cudaMemsetAsync(base + off, 0, s.bytes, upload));
                 }
             }
             off += align256(std::max<std::size_t>(s.bytes, 1));
         }
-        ASG_CUDA(cudaStreamSynchronize(stream));  // host sources go out of scope
+        ASG_CUDA(cudaStreamSynchronize(upload));  // host sources go out of scope
     }
 
     // Recording and spike-log buffers (mapped host memory, two parities).
@@ -688,6 +691,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     D.spike_log_cap = D.rec_spikes ? I.log_cap : 0;
     I.step = first;
     I.end = end;
+    ASG_TRY(finish_pending());
     I.id = next_id++;
     resident_bytes += total;
     *id_out = I.id;

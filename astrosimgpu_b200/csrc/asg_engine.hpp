@@ -144,6 +144,7 @@ private:
     // side-stream SIC batches (instances with InstDev::sic_side)
     static constexpr int kSideEvents = 8;
     cudaStream_t side = nullptr;
+    cudaStream_t upload = nullptr;  // table uploads of add(), beside the chunks in flight
     std::vector<Work> side_work;
     DevBuf d_side_work;
     int side_lead = 0, side_lead_max = 0;
