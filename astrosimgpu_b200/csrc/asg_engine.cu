@@ -4,6 +4,7 @@
 
 #include "asg_engine.hpp"
 
+#include <cub/cub.cuh>
 #include <omp.h>
 
 #include <algorithm>
@@ -74,77 +75,142 @@ AstroK make_astro_k(const asg_astro_params& a, double h, int substeps) {
     return k;
 }
 
-// Transposed in-edge structure of one set (host arrays).  A target's
-// in-edges are numbered p = 0.. in (source, row position) order; bit p of the
-// target's words marks an arrival on that edge.
-struct InRingHost {
-    std::vector<std::uint32_t> wbase;
-    std::vector<unsigned long long> edge;  // bit | target << 32 | dense << 57 | summary bit << 58
-    std::uint32_t words = 0;
+// Device memory from the stream-ordered allocator: freeing it does not wait
+// for the device (cudaFree would, and stall the chunks in flight).
+struct AsyncBuf {
+    void* p = nullptr;
+    cudaStream_t s = nullptr;
+    cudaError_t alloc(std::size_t bytes, cudaStream_t st) {
+        s = st;
+        return cudaMallocAsync(&p, std::max<std::size_t>(bytes, 16), st);
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+    ~AsyncBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
 };
 
-//
-// A stable counting sort by target, on the host's cores: thread k takes the
-// sources of a contiguous range (about m / T edges) and counts its edges per
-// target; per target, an exclusive prefix over the threads gives each
-// thread the number of that target's in-edges from earlier sources; each
-// thread then numbers its edges in (source, row position) order from there.
-// Every edge gets the number the one-thread pass would give it.
-InRingHost make_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std::uint32_t* tg,
-                        std::uint32_t n_targets) {
-    InRingHost r;
+// Transposed in-edge structure of one set, built on the device.  A target's
+// in-edges are numbered p = 0.. in (source, row position) order; bit p of the
+// target's words marks an arrival on that edge.
+struct InRingDev {
+    AsyncBuf wbase;  // [n_targets + 1] first bitmap word of each target
+    AsyncBuf edge;   // [m] bit | target << 32 | dense << 57 | summary bit << 58
+    std::uint32_t words = 0, m = 0;
+};
+
+__global__ void ring_count_kernel(const std::uint32_t* __restrict__ tg, std::uint32_t m,
+                                  std::uint32_t* __restrict__ deg) {
+    for (std::uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m;
+         e += gridDim.x * blockDim.x)
+        atomicAdd(deg + tg[e], 1u);
+}
+
+// words[t] = ceil(deg[t] / 32); words[n] = 0 (so the scan's last entry is the total)
+__global__ void ring_words_kernel(const std::uint32_t* __restrict__ deg, std::uint32_t n,
+                                  std::uint32_t* __restrict__ words) {
+    for (std::uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= n;
+         t += gridDim.x * blockDim.x)
+        words[t] = t < n ? (deg[t] + 31) / 32 : 0u;
+}
+
+__global__ void ring_iota_kernel(std::uint32_t* __restrict__ v, std::uint32_t m) {
+    for (std::uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m;
+         e += gridDim.x * blockDim.x)
+        v[e] = e;
+}
+
+// Sorted position i holds edge se[i] to target st[i]; the sort is stable, so
+// the edges of one target sit in (source, row position) order and the
+// edge's number is i - seg[t].
+__global__ void ring_pack_kernel(const std::uint32_t* __restrict__ st,
+                                 const std::uint32_t* __restrict__ se, std::uint32_t m,
+                                 const std::uint32_t* __restrict__ seg,
+                                 const std::uint32_t* __restrict__ wbase,
+                                 unsigned long long* __restrict__ edge) {
+    for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += gridDim.x * blockDim.x) {
+        const std::uint32_t t = st[i];
+        const std::uint32_t p = i - seg[t];
+        const std::uint32_t nw = wbase[t + 1] - wbase[t];
+        const std::uint32_t G = (nw + 63) / 64;
+        const unsigned long long bit = static_cast<unsigned long long>(wbase[t]) * 32 + p;
+        // A target of at most 32 words reads all its words at once and never
+        // its summary: its pushes skip the summary update.
+        const unsigned long long dense = nw <= 32 ? 1ull : 0ull;
+        edge[se[i]] = bit | (static_cast<unsigned long long>(t) << 32) | (dense << 57) |
+                      (static_cast<unsigned long long>((p / 32) / G) << 58);
+    }
+}
+
+// The in-edge numbering of one set (n_src sources, CSR rs / tg on the host)
+// on `st`: in-degrees, word bases and segment starts by exclusive scans,
+// then a stable radix sort of (target, edge) pairs and the packing.  Returns
+// with r.words known (the stream synchronised once for it).
+int build_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std::uint32_t* tg,
+                  std::uint32_t n_targets, cudaStream_t st, InRingDev& r) {
     const std::uint32_t m = rs[n_src];
-    const std::size_t n = std::max<std::uint32_t>(n_targets, 1);
-    // threads: one per 2^16 edges at most, and per-thread counters within 256 MB
-    int T = std::min<int>(omp_get_max_threads(), static_cast<int>(m >> 16));
-    T = std::max(1, std::min<int>(T, static_cast<int>((std::size_t{1} << 26) / n)));
-    std::vector<std::uint32_t> cut(static_cast<std::size_t>(T) + 1, n_src);
-    cut[0] = 0;
-    for (int k = 1; k < T; ++k) {  // first source whose row starts at or after k*m/T
-        const std::uint64_t e0 = static_cast<std::uint64_t>(m) * k / T;
-        cut[k] = static_cast<std::uint32_t>(std::lower_bound(rs, rs + n_src, e0) - rs);
-    }
-    std::vector<std::uint32_t> cnt(static_cast<std::size_t>(T) * n, 0);
-#pragma omp parallel for num_threads(T) schedule(static, 1)
-    for (int k = 0; k < T; ++k) {
-        std::uint32_t* h = cnt.data() + static_cast<std::size_t>(k) * n;
-        for (std::uint32_t e = rs[cut[k]]; e < rs[cut[k + 1]]; ++e) h[tg[e]]++;
-    }
-    r.wbase.assign(n_targets + 1, 0);
-    std::vector<std::uint32_t> deg(n_targets, 0);
-#pragma omp parallel for num_threads(T) schedule(static)
-    for (std::int64_t t = 0; t < static_cast<std::int64_t>(n_targets); ++t) {
-        std::uint32_t run = 0;
-        for (int k = 0; k < T; ++k) {
-            std::uint32_t& c = cnt[static_cast<std::size_t>(k) * n + static_cast<std::size_t>(t)];
-            const std::uint32_t v = c;
-            c = run;
-            run += v;
+    const std::uint32_t n = n_targets;
+    r.m = m;
+    if (m >= (1u << 31)) return fail(ASG_ERR_UNSUPPORTED, "a set of %u edges (at most 2^31-1)", m);
+    // Scratch beyond the arena: a failed allocation reports ASG_ERR_OOM (a
+    // server then waits for memory to free up).
+    auto need = [&](AsyncBuf& buf, std::size_t bytes) -> int {
+        const cudaError_t e = buf.alloc(bytes, st);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            return fail(ASG_ERR_OOM, "in-edge numbering: %zu device bytes unavailable", bytes);
         }
-        deg[static_cast<std::size_t>(t)] = run;
+        return e == cudaSuccess ? ASG_OK : cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
+    };
+    ASG_TRY(need(r.wbase, (static_cast<std::size_t>(n) + 1) * 4));
+    ASG_TRY(need(r.edge, static_cast<std::size_t>(m) * 8));
+    if (m == 0) {
+        ASG_CUDA(cudaMemsetAsync(r.wbase.p, 0, (static_cast<std::size_t>(n) + 1) * 4, st));
+        r.words = 0;
+        return ASG_OK;
     }
-    for (std::uint32_t t = 0; t < n_targets; ++t) r.wbase[t + 1] = r.wbase[t] + (deg[t] + 31) / 32;
-    r.words = r.wbase[n_targets];
-    r.edge.assign(m, 0);
-#pragma omp parallel for num_threads(T) schedule(static, 1)
-    for (int k = 0; k < T; ++k) {
-        std::uint32_t* next = cnt.data() + static_cast<std::size_t>(k) * n;
-        for (std::uint32_t s = cut[k]; s < cut[k + 1]; ++s) {
-            for (std::uint32_t e = rs[s]; e < rs[s + 1]; ++e) {
-                const std::uint32_t t = tg[e];
-                const std::uint32_t p = next[t]++;
-                const std::uint32_t nw = r.wbase[t + 1] - r.wbase[t];
-                const std::uint32_t G = (nw + 63) / 64;
-                const unsigned long long bit = static_cast<unsigned long long>(r.wbase[t]) * 32 + p;
-                // A target of at most 32 words reads all its words at once and
-                // never its summary: its pushes skip the summary update.
-                const unsigned long long dense = nw <= 32 ? 1ull : 0ull;
-                r.edge[e] = bit | (static_cast<unsigned long long>(t) << 32) | (dense << 57) |
-                            (static_cast<unsigned long long>((p / 32) / G) << 58);
-            }
-        }
-    }
-    return r;
+    AsyncBuf keys, keys_out, vals, vals_out, deg, seg, words, tmp;
+    for (AsyncBuf* buf : {&keys, &keys_out, &vals, &vals_out})
+        ASG_TRY(need(*buf, static_cast<std::size_t>(m) * 4));
+    for (AsyncBuf* buf : {&deg, &seg, &words})
+        ASG_TRY(need(*buf, (static_cast<std::size_t>(n) + 1) * 4));
+    ASG_CUDA(cudaMemcpyAsync(keys.p, tg, static_cast<std::size_t>(m) * 4, cudaMemcpyDefault, st));
+    ASG_CUDA(cudaMemsetAsync(deg.p, 0, (static_cast<std::size_t>(n) + 1) * 4, st));
+    const unsigned blocks = 4096;
+    ring_count_kernel<<<blocks, 256, 0, st>>>(keys.as<std::uint32_t>(), m, deg.as<std::uint32_t>());
+    ring_words_kernel<<<blocks, 256, 0, st>>>(deg.as<std::uint32_t>(), n, words.as<std::uint32_t>());
+    ring_iota_kernel<<<blocks, 256, 0, st>>>(vals.as<std::uint32_t>(), m);
+    ASG_CUDA(cudaGetLastError());
+    int end_bit = 1;
+    while (end_bit < 32 && (1ull << end_bit) < n) ++end_bit;
+    std::size_t b_scan = 0, b_sort = 0;
+    ASG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b_scan, deg.as<std::uint32_t>(),
+                                           seg.as<std::uint32_t>(), static_cast<int>(n) + 1, st));
+    ASG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b_sort, keys.as<std::uint32_t>(),
+                                             keys_out.as<std::uint32_t>(), vals.as<std::uint32_t>(),
+                                             vals_out.as<std::uint32_t>(), static_cast<int>(m), 0,
+                                             end_bit, st));
+    std::size_t b = std::max(b_scan, b_sort);
+    ASG_TRY(need(tmp, b));
+    ASG_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, b, deg.as<std::uint32_t>(),
+                                           seg.as<std::uint32_t>(), static_cast<int>(n) + 1, st));
+    b = std::max(b_scan, b_sort);
+    ASG_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, b, words.as<std::uint32_t>(),
+                                           r.wbase.as<std::uint32_t>(), static_cast<int>(n) + 1, st));
+    b = std::max(b_scan, b_sort);
+    ASG_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, b, keys.as<std::uint32_t>(),
+                                             keys_out.as<std::uint32_t>(), vals.as<std::uint32_t>(),
+                                             vals_out.as<std::uint32_t>(), static_cast<int>(m), 0,
+                                             end_bit, st));
+    ring_pack_kernel<<<blocks, 256, 0, st>>>(keys_out.as<std::uint32_t>(), vals_out.as<std::uint32_t>(),
+                                            m, seg.as<std::uint32_t>(), r.wbase.as<std::uint32_t>(),
+                                            r.edge.as<unsigned long long>());
+    ASG_CUDA(cudaGetLastError());
+    ASG_CUDA(cudaMemcpyAsync(&r.words, r.wbase.as<std::uint32_t>() + n, 4, cudaMemcpyDeviceToHost, st));
+    ASG_CUDA(cudaStreamSynchronize(st));
+    return ASG_OK;
 }
 
 // Compressed SIC lists in sliced ELL (32 targets per slice), each target's
@@ -524,9 +590,10 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     D.inv_tau_u = 1.0 / uval[2];
 
     // Host preprocessing of the tables.
-    InRingHost rex = make_in_ring(NE, rs_of(d.exc_primary), d.exc_primary.target, N);
-    InRingHost rin = make_in_ring(NI, rs_of(d.inh_primary), d.inh_primary.target, N);
-    InRingHost ras = make_in_ring(NE, rs_of(d.neuron_astro), d.neuron_astro.target, NA);
+    InRingDev rex, rin, ras;
+    ASG_TRY(build_in_ring(NE, rs_of(d.exc_primary), d.exc_primary.target, N, upload, rex));
+    ASG_TRY(build_in_ring(NI, rs_of(d.inh_primary), d.inh_primary.target, N, upload, rin));
+    ASG_TRY(build_in_ring(NE, rs_of(d.neuron_astro), d.neuron_astro.target, NA, upload, ras));
     // SIC parts: about kSicEdgesPerPart edges each, at most d_a2n - 1 (the
     // first part of arrival step A runs at step A - P and reads the factors
     // of step A - d_a2n, written by an earlier launch).
@@ -605,10 +672,10 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     add_seg(D.exc_rs, (NE + 1) * 4, d.exc_primary.n_sources ? d.exc_primary.row_start : zero_rs);
     add_seg(D.inh_rs, (NI + 1) * 4, d.inh_primary.n_sources ? d.inh_primary.row_start : zero_rs);
     add_seg(D.n2a_rs, (NE + 1) * 4, d.neuron_astro.n_sources ? d.neuron_astro.row_start : zero_rs);
-    auto ring_segs = [&](InRing& R, InRingHost& H, std::uint32_t n_t) {
+    auto ring_segs = [&](InRing& R, InRingDev& H, std::uint32_t n_t) {
         const std::size_t W = std::max<std::uint32_t>(H.words, 1);
-        add_seg(R.wbase, H.wbase.size() * 4, H.wbase.data());
-        add_seg(R.edge, H.edge.size() * 8, H.edge.data());
+        add_seg(R.wbase, (static_cast<std::size_t>(n_t) + 1) * 4, H.wbase.p);  // device copies
+        add_seg(R.edge, static_cast<std::size_t>(H.m) * 8, H.edge.p);
         const std::size_t T = std::max<std::uint32_t>(n_t, 1);
         add_seg(R.cnt, S * T * 4, nullptr);
         add_seg(R.lbit, S * T * kListCap * 4, nullptr);
@@ -649,7 +716,8 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
             *static_cast<void**>(s.dst) = base + off;
             if (s.bytes > 0) {
                 if (s.src != nullptr) {
-                    ASG_CUDA(cudaMemcpyAsync(base + off, s.src, s.bytes, cudaMemcpyHostToDevice,
+                    // host tables and the device-built rings alike (unified addressing)
+                    ASG_CUDA(cudaMemcpyAsync(base + off, s.src, s.bytes, cudaMemcpyDefault,
                                              upload));
                 } else {
                     ASG_CUDA(cudaMemsetAsync(base + off, 0, s.bytes, upload));
