@@ -5,7 +5,6 @@
 #include "asg_engine.hpp"
 
 #include <cub/cub.cuh>
-#include <omp.h>
 
 #include <algorithm>
 #include <cmath>
