@@ -47,3 +47,46 @@ def test_no_device_is_a_status_not_an_abort():
     d = m.desc()
     st = _lib.load().asg_create(C.byref(d), None, C.byref(opts), C.byref(h))
     assert st in (_lib.ASG_OK + 10, 3)  # ASG_ERR_NO_DEVICE (or a CUDA init error)
+
+
+# ctypes mirrors of the header's structs (astrosimgpu_b200/_lib.py), by C name.
+MIRRORS = {
+    "asg_neuron_params": "NeuronParams", "asg_astro_params": "AstroParams",
+    "asg_input": "InputParams", "asg_stp": "StpParams", "asg_csr": "Csr",
+    "asg_network_desc": "NetworkDesc", "asg_record_opts": "RecordOpts",
+    "asg_state": "State", "asg_engine_opts": "EngineOpts", "asg_serve_opts": "ServeOpts",
+    "asg_request_result": "RequestResult",
+}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Every ctypes mirror has the size and field offsets the C compiler gives
+    the header's struct (a field added on one side only would shift the
+    arguments the library reads)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "asg_b200.h"', "int main(void) {"]
+    for cname, pyname in MIRRORS.items():
+        st = getattr(_lib, pyname)
+        lines.append(f'printf("{pyname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in st._fields_:
+            lines.append(f'printf("{pyname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                               text=True).stdout.splitlines():
+        name, field, value = line.split()
+        got[(name, field)] = int(value)
+    for cname, pyname in MIRRORS.items():
+        st = getattr(_lib, pyname)
+        assert got[(pyname, "size")] == C.sizeof(st), pyname
+        for fname, _ in st._fields_:
+            assert got[(pyname, fname)] == getattr(st, fname).offset, (pyname, fname)
