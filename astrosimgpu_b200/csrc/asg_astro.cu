@@ -221,6 +221,13 @@ std::uint64_t bernoulli_threshold(double p) {
     return static_cast<std::uint64_t>(std::ceil(std::ldexp(p, 53)));
 }
 
+// Divisors taken through host-rounded reciprocals (div_by) must have a
+// magnitude in [2^-46, 2^63], the range where that division is exact.
+bool divisor_ok(double b) {
+    const double m = std::fabs(b);
+    return m >= 0x1p-46 && m <= 0x1p63;
+}
+
 AstroK make_astro_k(const double* c, double h_step, int substeps) {
     // c: Kd_IP3_1, Kd_IP3_2, Kd_act, Kd_inh, Km_SERCA, k_IP3R, rate_IP3R,
     //    rate_L, rate_SERCA, ratio_ER_cyt
@@ -337,6 +344,16 @@ int asg_astro_create(uint32_t n, const double* Ca, const double* IP3, const doub
     *out = nullptr;
     if (n > 0 && (Ca == nullptr || IP3 == nullptr || h == nullptr))
         return asg::fail(ASG_ERR_ARG, "asg_astro_create: state arrays are required");
+    // The per-cell parameters come as a set (the reference's cuda_astro_create
+    // takes all four): a partial set would leave the update reading a missing
+    // array.
+    const int n_params = (Ca_tot != nullptr) + (IP3_0 != nullptr) + (tau_IP3 != nullptr) +
+                         (delta_IP3 != nullptr);
+    if (n_params != 0 && n_params != 4)
+        return asg::fail(ASG_ERR_ARG,
+                         "asg_astro_create: give all four per-cell parameter arrays (Ca_tot, "
+                         "IP3_0, tau_IP3, delta_IP3) or none; %d of 4 given",
+                         n_params);
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         return asg::fail(ASG_ERR_NO_DEVICE, "asg_astro_create: no CUDA device");
@@ -365,7 +382,13 @@ int asg_astro_create(uint32_t n, const double* Ca, const double* IP3, const doub
     upload(e->tau, tau_IP3, false);
     if (tau_IP3 != nullptr) {
         std::vector<double> inv(n);
-        for (uint32_t i = 0; i < n; ++i) inv[i] = 1.0 / tau_IP3[i];
+        for (uint32_t i = 0; i < n && st == ASG_OK; ++i) {
+            if (!asg::divisor_ok(tau_IP3[i]))
+                st = asg::fail(ASG_ERR_UNSUPPORTED,
+                               "asg_astro_create: tau_IP3[%u] = %g outside [2^-46, 2^63]", i,
+                               tau_IP3[i]);
+            inv[i] = 1.0 / tau_IP3[i];
+        }
         upload(e->inv_tau, inv.data(), false);
     }
     upload(e->delta, delta_IP3, false);
@@ -460,6 +483,9 @@ int asg_astro_update(asg_astro* s, const double* consts, double h_step, int32_t 
     if (s == nullptr || consts == nullptr)
         return asg::fail(ASG_ERR_ARG, "asg_astro_update: NULL argument");
     if (substeps < 0) return asg::fail(ASG_ERR_ARG, "asg_astro_update: substeps < 0");
+    if (!asg::divisor_ok(consts[9]))
+        return asg::fail(ASG_ERR_UNSUPPORTED, "asg_astro_update: ratio_ER_cyt = %g outside "
+                         "[2^-46, 2^63]", consts[9]);
     auto* e = reinterpret_cast<AstroEngine*>(s);
     if (e->n == 0) return ASG_OK;
     if (e->Ca_tot.get() == nullptr) {
@@ -503,6 +529,9 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
         return asg::fail(ASG_ERR_ARG, "asg_astro_run_bernoulli: NULL argument");
     if (count < 0 || first < 0 || substeps < 0)
         return asg::fail(ASG_ERR_ARG, "asg_astro_run_bernoulli: negative step range");
+    if (!asg::divisor_ok(consts[9]) || (uniform && !asg::divisor_ok(tau_IP3)))
+        return asg::fail(ASG_ERR_UNSUPPORTED, "asg_astro_run_bernoulli: ratio_ER_cyt or tau_IP3 "
+                         "outside [2^-46, 2^63]");
     auto* e = reinterpret_cast<AstroEngine*>(s);
     if (!uniform && e->Ca_tot.get() == nullptr)
         return asg::fail(ASG_ERR_STATE, "asg_astro_run_bernoulli: no per-cell parameters");
@@ -673,8 +702,11 @@ extern "C" int asg_astro_autotune(asg_astro* s, const double* consts, double h_s
 // asg_astro_update_noalloc serves them: it updates caller-owned device arrays
 // in place and allocates nothing.  Its only scratch -- the correctly rounded
 // reciprocal of each cell's tau_IP3 that the division in the IP3 rate uses --
-// lives in the file-scope array below, which every GPU that loads this
-// library holds until the process exits.
+// lives in the file-scope array below.  The array is reserved with this
+// file's device code: when the module is loaded, i.e. at context creation
+// under eager module loading, or at the first call that needs the module
+// (the address lookup below) under CUDA's default lazy loading.  From then
+// on every GPU that uses the library holds it until the process exits.
 
 namespace asg {
 namespace {
@@ -683,7 +715,11 @@ constexpr std::uint32_t kNoAllocMaxCells = 1u << 20;  // 8 MiB of FP64 reciproca
 __device__ __align__(256) double g_noalloc_inv_tau[kNoAllocMaxCells];
 
 constexpr int kNoAllocMaxDevices = 64;
-double* g_noalloc_scratch[kNoAllocMaxDevices] = {};  // device address, per device
+struct ScratchAddr {
+    unsigned long long ctx_id = 0;  // driver id of the context the address belongs to
+    double* ptr = nullptr;
+};
+ScratchAddr g_noalloc_scratch[kNoAllocMaxDevices];  // per device ordinal
 std::mutex g_noalloc_mu;
 
 // inv_tau[i] = 1 / tau[i] (IEEE division: the correctly rounded reciprocal).
@@ -693,21 +729,60 @@ __global__ void noalloc_reciprocals(std::uint32_t n, const double* __restrict__ 
     if (i < n) inv_tau[i] = 1.0 / tau[i];
 }
 
-// Device address of the scratch array on the current device.  In host code
-// the array's name is only a host-side stand-in, so the address is looked up
-// once per device, with that device current, and cached.
-int noalloc_scratch(double** out) {
-    int dev = -1;
-    ASG_CUDA(cudaGetDevice(&dev));
+// Unique id of the context current on this thread (0 when none is current),
+// from the driver's cuCtxGetCurrent and cuCtxGetId, reached through the
+// runtime's entry-point query so the library need not link libcuda.  Ids are
+// never reused within a process, unlike context handles.
+int current_context_id(unsigned long long* id) {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (get_current == nullptr || get_id == nullptr) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1{}, q2{};
+        ASG_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1));
+        ASG_CUDA(cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2));
+        if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+            return fail(ASG_ERR_UNSUPPORTED, "driver lacks cuCtxGetCurrent/cuCtxGetId");
+        get_current = reinterpret_cast<GetCurrent>(f1);
+        get_id = reinterpret_cast<GetId>(f2);
+    }
+    void* ctx = nullptr;
+    *id = 0;
+    if (get_current(&ctx) != 0) return fail(ASG_ERR_CUDA, "cuCtxGetCurrent failed");
+    if (ctx != nullptr && get_id(ctx, id) != 0) return fail(ASG_ERR_CUDA, "cuCtxGetId failed");
+    return ASG_OK;
+}
+
+// Device address of the scratch array in the current device's context.  In
+// host code the array's name is only a host-side stand-in, so the address is
+// looked up with cudaGetSymbolAddress, with the device current, once per
+// device -- and again whenever the device's context is a new one (after
+// cudaDeviceReset, or after a host framework released and re-created the
+// primary context), because the cached address belongs to the old context.
+int noalloc_scratch(int dev, double** out) {
     if (dev < 0 || dev >= kNoAllocMaxDevices)
         return fail(ASG_ERR_UNSUPPORTED, "device ordinal %d beyond %d", dev, kNoAllocMaxDevices);
     std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (g_noalloc_scratch[dev] == nullptr) {
+    ScratchAddr& e = g_noalloc_scratch[dev];
+    unsigned long long ctx = 0;
+    ASG_TRY(current_context_id(&ctx));
+    if (e.ptr == nullptr || ctx == 0 || ctx != e.ctx_id) {
         void* p = nullptr;
-        ASG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_inv_tau));
-        g_noalloc_scratch[dev] = static_cast<double*>(p);
+        const cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_inv_tau);
+        if (ce == cudaErrorMemoryAllocation)
+            return fail(ASG_ERR_OOM,
+                        "asg_astro_update_noalloc: loading the module that holds the %u-cell "
+                        "(8 MiB) scratch array failed: device memory is exhausted",
+                        kNoAllocMaxCells);
+        ASG_CUDA(ce);
+        ASG_TRY(current_context_id(&ctx));  // the lookup made the context current
+        e.ctx_id = ctx;
+        e.ptr = static_cast<double*>(p);
     }
-    *out = g_noalloc_scratch[dev];
+    *out = e.ptr;
     return ASG_OK;
 }
 
@@ -733,17 +808,29 @@ extern "C" int asg_astro_update_noalloc(uint32_t n, double* Ca, double* IP3, dou
         consts == nullptr)
         return asg::fail(ASG_ERR_ARG, "asg_astro_update_noalloc: NULL argument");
     if (substeps < 0) return asg::fail(ASG_ERR_ARG, "asg_astro_update_noalloc: substeps < 0");
+    if (!asg::divisor_ok(consts[9]))
+        return asg::fail(ASG_ERR_UNSUPPORTED, "asg_astro_update_noalloc: ratio_ER_cyt = %g "
+                         "outside [2^-46, 2^63]", consts[9]);
     for (const void* p : {static_cast<const void*>(Ca), static_cast<const void*>(IP3),
                           static_cast<const void*>(h), static_cast<const void*>(ip3_input),
                           static_cast<const void*>(Ca_tot), static_cast<const void*>(IP3_0),
                           static_cast<const void*>(tau_IP3), static_cast<const void*>(delta_IP3)})
         if (reinterpret_cast<std::uintptr_t>(p) % alignof(double) != 0)
             return asg::fail(ASG_ERR_ARG, "asg_astro_update_noalloc: array not 8-byte aligned");
-    double* inv_tau = nullptr;
-    ASG_TRY(asg::noalloc_scratch(&inv_tau));
+    // A launch error is read back with cudaGetLastError, which would also
+    // return an error some earlier work left pending on this thread: refuse
+    // to run on top of one rather than report it as this call's failure.
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess)
+        return asg::fail(ASG_ERR_CUDA,
+                         "asg_astro_update_noalloc: a CUDA error from earlier work is pending "
+                         "on this thread (%s: %s); nothing was launched",
+                         cudaGetErrorName(pending), cudaGetErrorString(pending));
     int dev = 0, sms = 148;
     ASG_CUDA(cudaGetDevice(&dev));
     ASG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    double* inv_tau = nullptr;
+    ASG_TRY(asg::noalloc_scratch(dev, &inv_tau));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // Every entry this call reads is written first, in stream order, so the
     // previous call's contents never leak in.

@@ -131,11 +131,31 @@ static __device__ __noinline__ int poisson_large(std::uint64_t seed, std::uint64
 // correctly rounded a / b whenever y is the correctly rounded reciprocal and
 // no underflow or overflow occurs, i.e. it is bitwise the IEEE quotient the
 // reference computes, in three dependent operations instead of a full divide.
-__device__ __forceinline__ double div_by(double a, double b, double y) {
+//
+// The theorem's exclusions are kept off the fast path by the exponent of a
+// (an integer test): with 2^-959 <= |a| < 2^978 and a divisor of magnitude
+// in [2^-46, 2^63] (every divisor of the model is a time constant, a
+// capacitance, a slope factor or a volume ratio well inside it), the
+// quotient and the remainder are normal and the quotient is finite.  Every
+// other a -- tiny, huge, +-0 (whose quotient keeps a's sign), inf, NaN --
+// takes the IEEE division itself.  tests/div_by_check.cu checks the result
+// against IEEE division over random and edge-case operands of every class.
+__host__ __device__ __noinline__ inline double ieee_div(double a, double b) { return a / b; }
+
+__host__ __device__ __forceinline__ double div_by(double a, double b, double y) {
+#ifdef __CUDA_ARCH__
+    const unsigned biased = (static_cast<unsigned>(__double2hiint(a)) >> 20) & 0x7FFu;
+#else
+    std::uint64_t u;
+    __builtin_memcpy(&u, &a, sizeof u);
+    const unsigned biased = static_cast<unsigned>(u >> 52) & 0x7FFu;
+#endif
+    if (biased - 64u > 1936u) return ieee_div(a, b);  // biased exponent outside [64, 2000]
     const double q = a * y;
     const double r = fma(-q, b, a);
     return fma(r, y, q);
 }
+
 
 // ------------------------------------------------------ Li-Rinzel astrocyte
 

@@ -500,6 +500,40 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     ASG_TRY(check_uniform("neuron_astro", d.neuron_astro, NE, d.w_n2a, d.d_e_steps, d.stp));
     asg_stp nostp{};
     ASG_TRY(check_uniform("astro_neuron", d.astro_neuron, NA, d.w_a2n, d.d_a2n_steps, nostp));
+    // Divisors taken through their host-rounded reciprocals (div_by) must lie
+    // in the range where that division is exact: magnitudes in [2^-46, 2^63].
+    {
+        auto divisor_ok = [](double b) {
+            const double m = std::fabs(b);
+            return m >= 0x1p-46 && m <= 0x1p63;
+        };
+        const std::pair<const char*, double> neuron_div[] = {
+            {"neuron_exc.C_m", d.exc.C_m},         {"neuron_exc.Delta_T", d.exc.Delta_T},
+            {"neuron_exc.tau_w", d.exc.tau_w},     {"neuron_inh.C_m", d.inh.C_m},
+            {"neuron_inh.Delta_T", d.inh.Delta_T}, {"neuron_inh.tau_w", d.inh.tau_w}};
+        const std::pair<const char*, double> astro_div[] = {
+            {"astrocyte.ratio_ER_cyt", d.astro.ratio_ER_cyt},
+            {"astrocyte.tau_IP3", d.tau_IP3 == nullptr ? d.tau_IP3_u : 1.0}};
+        for (const auto& dv : neuron_div)
+            if (N > 0 && !divisor_ok(dv.second))
+                return fail(ASG_ERR_UNSUPPORTED, "%s = %g outside [2^-46, 2^63]", dv.first,
+                            dv.second);
+        for (const auto& dv : astro_div)
+            if (NA > 0 && !divisor_ok(dv.second))
+                return fail(ASG_ERR_UNSUPPORTED, "%s = %g outside [2^-46, 2^63]", dv.first,
+                            dv.second);
+        if (d.stp.enabled && !divisor_ok(d.stp.tau_rec))
+            return fail(ASG_ERR_UNSUPPORTED, "stp.tau_rec = %g outside [2^-46, 2^63]",
+                        d.stp.tau_rec);
+        if (d.stp.enabled && d.stp.tau_fac >= 1e-10 && !divisor_ok(d.stp.tau_fac))
+            return fail(ASG_ERR_UNSUPPORTED, "stp.tau_fac = %g outside [2^-46, 2^63]",
+                        d.stp.tau_fac);
+        if (d.tau_IP3 != nullptr)
+            for (std::uint32_t a = 0; a < NA; ++a)
+                if (!divisor_ok(d.tau_IP3[a]))
+                    return fail(ASG_ERR_UNSUPPORTED, "tau_IP3[%u] = %g outside [2^-46, 2^63]", a,
+                                d.tau_IP3[a]);
+    }
 
     auto inst = std::make_unique<Instance>();
     Instance& I = *inst;

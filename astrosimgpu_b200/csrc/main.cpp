@@ -25,8 +25,9 @@ namespace {
 
 void usage(const char* argv0) {
     std::cout << "Usage: " << argv0 << " [options]\n\n"
-              << "Simulates a tripartite neuron-astrocyte network on the B200 and reports\n"
-              << "the calcium and spiking statistics used to assess synchronisation.\n\n"
+              << "Runs the neuron-astrocyte model of a JSON parameter file with every\n"
+              << "timestep on one B200 GPU, writes the spike and trace files, and prints\n"
+              << "the firing and astrocyte-calcium summary.\n\n"
               << "Options:\n"
               << "  -c, --config PATH     parameter file (JSON)   [config/use_case.json]\n"
               << "  -o, --output DIR      output directory        [from config]\n"

@@ -339,27 +339,3 @@ class Server:
         except Exception:
             pass
 
-
-def smoke_check():
-    """A short quick.json run on cuda:0 against the reference (smoke())."""
-    from oracle import ref
-    path = config_path("quick")
-    m = Model(path, pre_time=0.0)
-    net = Network(m, record=_lib.RecordOpts(0, 10, 1, 0, 0))
-    net.step(300)
-    st, src = net.fetch_spikes()
-    if ref.ref_available():
-        r = ref.RefNetwork(path=path, pre_time=0.0)
-        rs, rsrc = r.run(300)
-        rstate = r.state()
-    else:
-        from oracle import config as oc
-        p = oc.PortNetwork(oc.load(path))
-        rs, rsrc = p.run(300)
-        rstate = p.state()
-    if not (np.array_equal(st, rs) and np.array_equal(src, rsrc)):
-        raise AssertionError("network spikes differ from the oracle over 300 steps")
-    g = net.state()
-    for k in ("V", "Ca", "IP3", "h"):
-        if not np.allclose(g[k], rstate[k], rtol=1e-12, atol=1e-12):
-            raise AssertionError(f"network state {k} differs from the oracle")

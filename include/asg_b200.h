@@ -324,10 +324,17 @@ int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels);
  * is consumed and zeroed).  `stream` is a cudaStream_t (NULL: the default
  * stream); the call is asynchronous on it.  The only scratch, one double per
  * cell, lives in a static device array of at most 1,048,576 cells: larger n
- * is rejected with ASG_ERR_ARG.  Nothing is allocated, not even on the first
- * call; that first call on a device looks up the array's device address, so
- * make it before any stream capture.  Every call shares the array: calls that
- * overlap on the GPU race and must be ordered by the caller. */
+ * is rejected with ASG_ERR_ARG.  The call allocates nothing itself.  The
+ * 8 MiB array is reserved together with the library's device code when CUDA
+ * loads that module: at context creation under eager module loading, or, under
+ * CUDA's default lazy loading, during the first call on a device; if device
+ * memory is already exhausted then, that call returns ASG_ERR_OOM.  The first
+ * call on a device (and the first after that device's context was re-created,
+ * e.g. by cudaDeviceReset) looks up the array's device address, so make it
+ * before any stream capture.  The call refuses to launch (ASG_ERR_CUDA) while
+ * an earlier CUDA error is pending on the calling thread.  Every call shares
+ * the array: calls that overlap on the GPU race and must be ordered by the
+ * caller. */
 int asg_astro_update_noalloc(uint32_t n, double* Ca, double* IP3, double* h, double* ip3_input,
                              const double* Ca_tot, const double* IP3_0, const double* tau_IP3,
                              const double* delta_IP3, const double* consts, double h_step,

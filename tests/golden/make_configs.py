@@ -4,7 +4,7 @@ The engine reads the reference's own JSON schema.  The parameter values of
 the shipped model configurations are the inputs the parity tests and the
 benchmark run on, so they are carried over as plain JSON (comments and prose
 dropped, keys and numbers unchanged).  Run in a checkout that has the
-reference at REF (default /root/reference).  Two derived files follow the
+reference sources named by the environment variable ASTROSIMGPU_REF.  Two derived files follow the
 benchmark shapes: paper_sparse_dt005 (dt 0.05 ms, 1.5 ms delays, config C2)
 and c0_literal (use_case with p_primary 0.1, every excitatory synapse
 recruiting from a random pool of 100, 1.5 ms delays).
@@ -14,7 +14,7 @@ import os
 import re
 import sys
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("ASTROSIMGPU_REF")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..",
                    "astrosimgpu_b200", "configs")
 
@@ -24,6 +24,8 @@ def strip_comments(text: str) -> str:
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "config")):
+        sys.exit("set ASTROSIMGPU_REF to the reference checkout (the directory holding config/)")
     os.makedirs(OUT, exist_ok=True)
     names = ["use_case", "bursting", "quick", "paper_sparse", "kernel_scaling", "no_spiking",
              "random_pool", "scale_1000"]

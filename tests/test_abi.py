@@ -90,3 +90,19 @@ def test_struct_layouts_match_header(tmp_path):
         assert got[(pyname, "size")] == C.sizeof(st), pyname
         for fname, _ in st._fields_:
             assert got[(pyname, fname)] == getattr(st, fname).offset, (pyname, fname)
+
+
+def test_astro_create_rejects_a_partial_parameter_set():
+    """All four per-cell parameter arrays or none: a partial set is refused on
+    the host (before any device work), so no update can read a missing array."""
+    import numpy as np
+    lib = _lib.load()
+    n = 8
+    a = [np.ones(n) for _ in range(7)]
+    h = C.c_void_p()
+    for missing in range(3, 7):
+        args = [_lib.dptr(x) if i != missing else None for i, x in enumerate(a)]
+        st = lib.asg_astro_create(n, *args, C.byref(h))
+        assert st == 1, missing  # ASG_ERR_ARG
+        assert b"all four per-cell parameter arrays" in lib.asg_last_error()
+        assert not h.value

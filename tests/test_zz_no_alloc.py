@@ -23,38 +23,53 @@ def dev(a):
 
 
 def test_noalloc_matches_regular_entry_point_twice():
+    """Two calls in a row with different tau_IP3 arrays and sizes: the second
+    call's reciprocals must be recomputed over the shared scratch array, so a
+    stale entry left by the first call would change its result."""
     import torch
     rng = np.random.default_rng(11)
-    n = 5003
-    w = ScalingWorkload(n)
+    n1, n2 = 5003, 4001
+    w = ScalingWorkload(n1)
     Ca, IP3, h = w.initial_state()
-    Ca_tot = w.Ca_tot * (1 + 0.05 * rng.standard_normal(n))
-    IP3_0 = w.IP3_0 * (1 + 0.05 * rng.standard_normal(n))
-    tau = w.tau_IP3 * (1 + 0.05 * rng.standard_normal(n))
-    delta = w.delta_IP3 * (1 + 0.05 * rng.standard_normal(n))
-    inputs = [np.where(rng.random(n) < 0.3, rng.random(n), 0.0) for _ in range(2)]
+    Ca_tot = w.Ca_tot * (1 + 0.05 * rng.standard_normal(n1))
+    IP3_0 = w.IP3_0 * (1 + 0.05 * rng.standard_normal(n1))
+    delta = w.delta_IP3 * (1 + 0.05 * rng.standard_normal(n1))
+    taus = [w.tau_IP3 * (1 + 0.05 * rng.standard_normal(n1)),
+            w.tau_IP3 * (0.5 + rng.random(n1))]  # a different array for call 2
+    inputs = [np.where(rng.random(n1) < 0.3, rng.random(n1), 0.0) for _ in range(2)]
 
-    regular = AstroBackend(Ca, IP3, h, Ca_tot, IP3_0, tau, delta)
-    d = {k: dev(v) for k, v in dict(Ca=Ca, IP3=IP3, h=h, Ca_tot=Ca_tot, IP3_0=IP3_0, tau=tau,
-                                       delta=delta, inp=np.zeros(n)).items()}
+    d = {k: dev(v) for k, v in dict(Ca=Ca, IP3=IP3, h=h, Ca_tot=Ca_tot, IP3_0=IP3_0,
+                                       delta=delta, inp=np.zeros(n1)).items()}
     lib = _lib.load()
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    for call, inp in enumerate(inputs):
-        regular.push_input(inp)
+    state = (Ca, IP3, h)
+    for call, (n, tau, inp) in enumerate(zip((n1, n2), taus, inputs)):
+        # the regular entry point on the state both paths hold before this call
+        regular = AstroBackend(*[a[:n].copy() for a in state], Ca_tot[:n].copy(),
+                               IP3_0[:n].copy(), tau[:n].copy(), delta[:n].copy())
+        regular.push_input(inp[:n].copy())
         regular.update(w.consts, w.h_step, 2)
+        rCa, rIP3, rh = regular.pull_state()
+        regular.destroy()
+        d_tau = dev(tau)
         d["inp"].copy_(torch.from_numpy(inp))
         st = lib.asg_astro_update_noalloc(
             n, *[C.c_void_p(d[k].data_ptr()) for k in ("Ca", "IP3", "h", "inp", "Ca_tot",
-                                                         "IP3_0", "tau", "delta")],
+                                                         "IP3_0")],
+            C.c_void_p(d_tau.data_ptr()), C.c_void_p(d["delta"].data_ptr()),
             _lib.dptr(w.consts), w.h_step, 2, 0.0, 1, 0.0, 0, 0, stream)
         assert st == 0, lib.asg_last_error()
         torch.cuda.synchronize()
-        rCa, rIP3, rh = regular.pull_state()
-        assert np.array_equal(d["Ca"].cpu().numpy(), rCa), call
-        assert np.array_equal(d["IP3"].cpu().numpy(), rIP3), call
-        assert np.array_equal(d["h"].cpu().numpy(), rh), call
-        assert not d["inp"].any()  # the input is consumed, as the regular path does
-    regular.destroy()
+        gCa, gIP3, gh = (d[k].cpu().numpy() for k in ("Ca", "IP3", "h"))
+        assert np.array_equal(gCa[:n], rCa), call
+        assert np.array_equal(gIP3[:n], rIP3), call
+        assert np.array_equal(gh[:n], rh), call
+        # cells beyond n are not touched, and the input is consumed (zeroed)
+        # over [0, n) only, as the regular path does for its cells
+        for g, before in zip((gCa, gIP3, gh), state):
+            assert np.array_equal(g[n:], before[n:]), call
+        assert not d["inp"][:n].any()
+        state = (gCa.copy(), gIP3.copy(), gh.copy())
 
 
 def test_pipelined_ranges_with_noise_match_single_launch():
