@@ -44,7 +44,15 @@ struct UniformParams {
     double Ca_tot, IP3_0, tau, delta, inv_tau;
 };
 
-enum InputMode { kInputArray = 0, kInputBernoulli = 1 };
+// Where a step's IP3 input comes from:
+//   kInputArrayZero  the input array, zeroed after use (the reference kernel's
+//                    contract; the allocation-free entry point, whose array
+//                    belongs to the caller)
+//   kInputBernoulli  generated on the device (the kernel-scaling workload)
+//   kInputArray      the input array, left as it is: the resident engine
+//                    knows the caller's next push overwrites all of it
+//   kInputNone       zero input (no push since the last update), not read
+enum InputMode { kInputArrayZero = 0, kInputBernoulli = 1, kInputArray = 2, kInputNone = 3 };
 
 struct StepArgs {
     std::int64_t n;
@@ -76,6 +84,8 @@ __device__ __forceinline__ void advance_cell(const StepArgs& a, const AstroArray
                     1000ULL + static_cast<std::uint64_t>(step)) >> 11) < a.p_threshold
                  ? a.weight
                  : 0.0;
+    } else if (kInput == kInputNone) {
+        in = 0.0;
     } else {
         in = s.input[i];
     }
@@ -125,7 +135,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) astro_step_kernel(StepArgs
             Ca2[2 * q + 1] = ca1;
             IP32[2 * q + 1] = ip31;
             h2[2 * q + 1] = hh1;
-            if (kInput == kInputArray) {
+            if (kInput == kInputArrayZero) {
                 reinterpret_cast<double2*>(s.input)[2 * q] = make_double2(0.0, 0.0);
                 reinterpret_cast<double2*>(s.input)[2 * q + 1] = make_double2(0.0, 0.0);
             }
@@ -138,7 +148,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) astro_step_kernel(StepArgs
             s.Ca[i] = ca;
             s.IP3[i] = ip3;
             s.h[i] = hh;
-            if (kInput == kInputArray) s.input[i] = 0.0;
+            if (kInput == kInputArrayZero) s.input[i] = 0.0;
         }
     } else if (kCells == 2) {
         const std::int64_t pairs = a.n / 2;
@@ -154,7 +164,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) astro_step_kernel(StepArgs
             Ca2[p] = ca;
             IP32[p] = ip3;
             h2[p] = hh;
-            if (kInput == kInputArray)
+            if (kInput == kInputArrayZero)
                 reinterpret_cast<double2*>(s.input)[p] = make_double2(0.0, 0.0);
         }
         // Odd tail cell.
@@ -165,7 +175,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) astro_step_kernel(StepArgs
             s.Ca[i] = ca;
             s.IP3[i] = ip3;
             s.h[i] = hh;
-            if (kInput == kInputArray) s.input[i] = 0.0;
+            if (kInput == kInputArrayZero) s.input[i] = 0.0;
         }
     } else {
         for (std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -175,7 +185,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) astro_step_kernel(StepArgs
             s.Ca[i] = ca;
             s.IP3[i] = ip3;
             s.h[i] = hh;
-            if (kInput == kInputArray) s.input[i] = 0.0;
+            if (kInput == kInputArrayZero) s.input[i] = 0.0;
         }
     }
 }
@@ -262,6 +272,20 @@ struct AstroEngine {
     double last_ms = 0.0;
     std::int64_t last_kernels = 0;
     int shape = 0;  // launch shape (see kShapes), set by asg_astro_autotune
+    // Per-cell parameters given at create.  When every cell has the same four
+    // values (bit for bit) they are kept as scalars and no array is read.
+    bool has_params = false;
+    bool params_uniform = false;
+    UniformParams up{};
+    // A push since the last update: the update reads the input array.  With
+    // none, the input is zero (the reference kernel zeroes it after use) and
+    // is not read; the engine never writes it, since each push overwrites
+    // the whole array.
+    bool input_pending = false;
+    // Device time of consecutive asg_astro_update calls: ev0 is recorded by
+    // the first update after the last timing read, ev1 by every update.
+    bool upd_armed = false;
+    std::int64_t upd_calls = 0;
     // Captured chunk of Bernoulli steps, rebuilt when its arguments change.
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
@@ -377,6 +401,23 @@ int asg_astro_create(uint32_t n, const double* Ca, const double* IP3, const doub
     upload(e->IP3, IP3, true);
     upload(e->h, h, true);
     upload(e->input, nullptr, true);
+    e->has_params = n_params == 4;
+    if (e->has_params && n > 0) {
+        auto same = [n](const double* v) {
+            for (uint32_t i = 1; i < n; ++i)
+                if (std::memcmp(&v[i], &v[0], sizeof(double)) != 0) return false;
+            return true;
+        };
+        e->params_uniform = same(Ca_tot) && same(IP3_0) && same(tau_IP3) && same(delta_IP3);
+        if (e->params_uniform) {
+            if (!asg::divisor_ok(tau_IP3[0]))
+                st = asg::fail(ASG_ERR_UNSUPPORTED,
+                               "asg_astro_create: tau_IP3 = %g outside [2^-46, 2^63]", tau_IP3[0]);
+            e->up = asg::UniformParams{Ca_tot[0], IP3_0[0], tau_IP3[0], delta_IP3[0],
+                                       1.0 / tau_IP3[0]};
+            Ca_tot = IP3_0 = tau_IP3 = delta_IP3 = nullptr;  // nothing per cell to upload
+        }
+    }
     upload(e->Ca_tot, Ca_tot, false);
     upload(e->IP3_0, IP3_0, false);
     upload(e->tau, tau_IP3, false);
@@ -455,6 +496,7 @@ int asg_astro_push_input(asg_astro* s, const double* ip3_input) {
                                  cudaMemcpyHostToDevice, e->h2d));
         ASG_CUDA(cudaEventRecord(e->ev_in[c], e->h2d));
     }
+    e->input_pending = true;
     return ASG_OK;
 }
 
@@ -488,35 +530,53 @@ int asg_astro_update(asg_astro* s, const double* consts, double h_step, int32_t 
                          "[2^-46, 2^63]", consts[9]);
     auto* e = reinterpret_cast<AstroEngine*>(s);
     if (e->n == 0) return ASG_OK;
-    if (e->Ca_tot.get() == nullptr) {
+    if (!e->has_params) {
         return asg::fail(ASG_ERR_STATE,
                          "asg_astro_update: per-cell parameters were not given at create");
     }
     asg::StepArgs a{};
     a.n = e->n;
     a.k = asg::make_astro_k(consts, h_step, substeps);
+    a.u = e->up;
     a.noise_std = noise_std;
     a.independent = independent_noise;
     a.shared_noise = shared_noise;
     a.noise_seed = noise_seed;
     a.noise_index = noise_index;
     a.step_base = e->step_base.as<std::int64_t>();
-    ASG_CUDA(cudaEventRecord(e->ev0, e->stream));
+    if (!e->upd_armed) {
+        ASG_CUDA(cudaEventRecord(e->ev0, e->stream));
+        e->upd_armed = true;
+        e->upd_calls = 0;
+    }
     // The reference applies noise only when noise_std > 0 (astrocyte.cpp:
     // 313-322); otherwise the caller's shared value (0) enters the RHS.
     if (!(noise_std > 0.0)) a.independent = 0;
+    const bool pending = e->input_pending;
     for (int c = 0; c < e->pieces(); ++c) {
         const std::int64_t b = e->piece_begin(c);
         ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_in[c], 0));   // this range's input
         ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_out[c], 0));  // last Ca copy read it
         a.n = e->piece_end(c) - b;
         a.i0 = b;
-        ASG_CUDA((asg::launch_astro<false, asg::kInputArray, true>(e->shape, e->sms, a,
-                                                                    e->arrays_at(b), e->stream)));
+        const asg::AstroArrays arr = e->arrays_at(b);
+        cudaError_t le;
+        if (e->params_uniform)
+            le = pending ? asg::launch_astro<true, asg::kInputArray, true>(e->shape, e->sms, a, arr,
+                                                                          e->stream)
+                         : asg::launch_astro<true, asg::kInputNone, true>(e->shape, e->sms, a, arr,
+                                                                         e->stream);
+        else
+            le = pending ? asg::launch_astro<false, asg::kInputArray, true>(e->shape, e->sms, a,
+                                                                           arr, e->stream)
+                         : asg::launch_astro<false, asg::kInputNone, true>(e->shape, e->sms, a,
+                                                                          arr, e->stream);
+        ASG_CUDA(le);
         ASG_CUDA(cudaEventRecord(e->ev_k[c], e->stream));
     }
+    e->input_pending = false;
     ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
-    e->last_kernels = 1;
+    e->upd_calls += e->pieces();
     return ASG_OK;
 }
 
@@ -533,8 +593,17 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
         return asg::fail(ASG_ERR_UNSUPPORTED, "asg_astro_run_bernoulli: ratio_ER_cyt or tau_IP3 "
                          "outside [2^-46, 2^63]");
     auto* e = reinterpret_cast<AstroEngine*>(s);
-    if (!uniform && e->Ca_tot.get() == nullptr)
+    if (!uniform && !e->has_params)
         return asg::fail(ASG_ERR_STATE, "asg_astro_run_bernoulli: no per-cell parameters");
+    e->upd_armed = false;
+    // Per-cell parameters that are all equal run as the scalars they are.
+    if (!uniform && e->params_uniform) {
+        uniform = 1;
+        Ca_tot = e->up.Ca_tot;
+        IP3_0 = e->up.IP3_0;
+        tau_IP3 = e->up.tau;
+        delta_IP3 = e->up.delta;
+    }
     if (e->n == 0 || count == 0) {
         e->last_ms = 0.0;
         e->last_kernels = 0;
@@ -616,6 +685,15 @@ int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels) {
     asg::clear_error();
     if (s == nullptr) return asg::fail(ASG_ERR_ARG, "asg_astro_last_timing: NULL handle");
     auto* e = reinterpret_cast<AstroEngine*>(s);
+    if (e->upd_armed) {
+        // updates since the last read: ev0 of the first .. ev1 of the last
+        ASG_CUDA(cudaEventSynchronize(e->ev1));
+        float ms = 0.0f;
+        ASG_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+        e->last_ms = ms;
+        e->last_kernels = e->upd_calls;
+        e->upd_armed = false;
+    }
     if (device_ms) *device_ms = e->last_ms;
     if (kernels) *kernels = e->last_kernels;
     return ASG_OK;
@@ -848,6 +926,6 @@ extern "C" int asg_astro_update_noalloc(uint32_t n, double* Ca, double* IP3, dou
     const asg::AstroArrays arr{Ca, IP3, h, ip3_input, Ca_tot, IP3_0, tau_IP3, inv_tau, delta_IP3};
     // Shape 1: one cell per thread with 8-byte accesses, so caller arrays need
     // no more than double alignment.
-    ASG_CUDA((asg::launch_astro<false, asg::kInputArray, true>(1, sms, a, arr, st)));
+    ASG_CUDA((asg::launch_astro<false, asg::kInputArrayZero, true>(1, sms, a, arr, st)));
     return ASG_OK;
 }

@@ -277,7 +277,10 @@ int asg_serve_destroy(asg_server* s);
 /* -------------------------------------- astrocyte backend (drop-in)
  * Same four movement points as the reference's native CUDA backend
  * (astrocyte_cuda.hpp:15-27): create with resident state, push the step's
- * input, update, pull calcium, destroy with the state copied back. */
+ * input, update, pull calcium, destroy with the state copied back.
+ * As in the reference, an update consumes the pushed input: an update with
+ * no push since the previous one sees zero input.  Per-cell parameter
+ * arrays whose entries are all equal are held as scalars. */
 typedef struct asg_astro asg_astro;
 
 int asg_astro_create(uint32_t n, const double* Ca, const double* IP3, const double* h,
@@ -312,7 +315,9 @@ int asg_astro_autotune(asg_astro* s, const double* consts, double h_step, int32_
  * handle; ASG_ERR_ARG names the valid range.  Every shape gives the same
  * bits.  No counterpart in the reference (a tuning knob, like autotune). */
 int asg_astro_set_shape(asg_astro* s, int32_t shape);
-/* Device ms of the last run call and kernels launched. */
+/* Device ms and kernels launched of the last asg_astro_run_bernoulli call,
+ * or of all asg_astro_update calls since the previous timing read (waits for
+ * them to finish). */
 int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels);
 
 /* Allocation-free astrocyte update.  No counterpart in the reference: it

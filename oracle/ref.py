@@ -66,6 +66,9 @@ def ref():
         lib.ref_net_run.restype = C.c_int64
         lib.ref_net_run.argtypes = [C.c_void_p, C.c_int64, C.c_int64, I64, U32, C.c_int64]
         lib.ref_net_sic_factors.argtypes = [C.c_void_p, D]
+        lib.ref_net_set_state.argtypes = [C.c_void_p, D, I32, D]
+        lib.ref_net_load_table.restype = C.c_int
+        lib.ref_net_load_table.argtypes = [C.c_void_p, C.c_int, C.c_int64, U32, U32]
         lib.ref_rng_bits.restype = C.c_uint64
         lib.ref_rng_bits.argtypes = [C.c_uint64] * 3
         lib.ref_rng_uniform.restype = C.c_double
@@ -186,6 +189,26 @@ class RefNetwork:
             raise RuntimeError("spike buffer too small")
         self.step += count
         return st[:total], src[:total]
+
+    def set_state(self, st):
+        """Overwrite the dynamic state (dict with the keys of state())."""
+        keys = ("V", "w", "g_ex", "dg_ex", "g_in", "dg_in", "I_sic")
+        n7 = np.ascontiguousarray(np.concatenate([np.asarray(st[k], np.float64) for k in keys]))
+        refr = np.ascontiguousarray(st["refractory"], np.int32)
+        a3 = np.ascontiguousarray(np.concatenate([np.asarray(st[k], np.float64)
+                                                  for k in ("Ca", "IP3", "h")]))
+        ref().ref_net_set_state(self.h, _dp(n7), refr.ctypes.data_as(I32), _dp(a3))
+
+    def load_table(self, which: int, row_start, target):
+        """Replace connection set `which` by the CSR (row_start, target)."""
+        rs = np.ascontiguousarray(row_start, np.uint32)
+        tg = np.ascontiguousarray(target, np.uint32)
+        if len(tg) == 0:
+            tg = np.zeros(1, np.uint32)
+        rc = ref().ref_net_load_table(self.h, which, len(rs) - 1, rs.ctypes.data_as(U32),
+                                      tg.ctypes.data_as(U32))
+        if rc != 0:
+            raise ValueError(f"table {which}: {len(rs) - 1} rows do not match the set's sources")
 
     def sic_factors(self):
         out = np.zeros(self.n_astro)

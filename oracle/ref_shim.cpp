@@ -20,6 +20,7 @@
 #include "astrosimgpu/astrocyte_kernel.hpp"
 #undef private
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -262,6 +263,71 @@ std::int64_t ref_net_run(void* h, std::int64_t first, std::int64_t count, std::i
 void ref_net_sic_factors(void* h, double* out) {
     auto* r = static_cast<RefNet*>(h);
     for (index_t a = 0; a < r->net->astro_.size(); ++a) out[a] = r->net->astro_.sic_factor(a);
+}
+
+// Overwrites the dynamic state (the layout of ref_net_state).  Used to start
+// the reference from a state another simulator reached, or to perturb it.
+void ref_net_set_state(void* h, const double* neuron7, const std::int32_t* refractory,
+                       const double* astro3) {
+    auto* r = static_cast<RefNet*>(h);
+    NeuronPopulation& n = r->net->neurons_;
+    const std::size_t N = n.V_.size();
+    vec<real>* arrs[7] = {&n.V_, &n.w_, &n.g_ex_, &n.dg_ex_, &n.g_in_, &n.dg_in_, &n.I_sic_};
+    for (int k = 0; k < 7; ++k) std::memcpy(arrs[k]->data(), neuron7 + k * N, N * 8);
+    std::memcpy(n.refractory_steps_.data(), refractory, N * 4);
+    AstrocytePopulation& a = r->net->astro_;
+    const std::size_t NA = a.Ca_.size();
+    std::memcpy(a.Ca_.data(), astro3, NA * 8);
+    std::memcpy(a.IP3_.data(), astro3 + NA, NA * 8);
+    std::memcpy(a.h_.data(), astro3 + 2 * NA, NA * 8);
+}
+
+// Replaces connection set `which` (0 exc, 1 inh, 2 neuron->astro, 3
+// astro->neuron) by another CSR grouped by source -- e.g. the product's
+// fixed-in-degree tables, which the reference's Bernoulli builder cannot
+// make -- with the set's uniform weight and delay and fresh STP state (the
+// set's own finalise, as build_primary_connections does), then re-derives
+// what Network::build computes from the sets (network.cpp:64-98): the edge
+// counts, the SIC sources and the astrocyte input sinks.  Returns 0, or -1
+// when the row count does not match the set's sources.
+int ref_net_load_table(void* h, int which, std::int64_t n_rows, const std::uint32_t* row_start,
+                       const std::uint32_t* target) {
+    auto* r = static_cast<RefNet*>(h);
+    Network& net = *r->net;
+    const ModelConfig& c = net.cfg_;
+    const index_t sources[4] = {c.N.N_exc, c.N.N_inh, c.N.N_exc, c.N.N_astro};
+    if (which < 0 || which > 3 || n_rows != static_cast<std::int64_t>(sources[which])) return -1;
+    ConnectionSet& set = set_of(r, which);
+    const std::size_t m = row_start[n_rows];
+    set = ConnectionSet{};
+    set.row_start.assign(row_start, row_start + n_rows + 1);
+    set.target.assign(target, target + m);
+    const double weights[4] = {c.syn.w_e, c.syn.w_i, c.syn.w_n2a, c.syn.w_a2n};
+    const double delays_ms[4] = {c.syn.d_e, c.syn.d_i, c.syn.d_e, c.syn.d_a2n};
+    const int delay = std::max(1, static_cast<int>(delays_ms[which] / c.time.dt + 0.5));
+    set.weight.assign(m, weights[which]);
+    set.delay_steps.assign(m, delay);
+    StpParams none;
+    none.enabled = false;
+    set.finalise(sources[which], which == 3 ? none : c.syn.stp);
+
+    net.stats_.n_primary_exc = net.exc_primary_.size();
+    net.stats_.n_primary_inh = net.inh_primary_.size();
+    net.stats_.n_neuron_to_astro = net.neuron_astro_.size();
+    net.stats_.n_astro_to_neuron = net.astro_neuron_.size();
+    net.sic_sources_.clear();
+    for (index_t a = 0; a < c.N.N_astro; ++a)
+        if (net.astro_neuron_.row_start[a] < net.astro_neuron_.row_start[a + 1])
+            net.sic_sources_.push_back(a);
+    vec<char> seen(c.N.N_astro, 0);
+    net.astro_input_sinks_.clear();
+    for (const index_t t : net.neuron_astro_.target)
+        if (!seen[t]) {
+            seen[t] = 1;
+            net.astro_input_sinks_.push_back(t);
+        }
+    std::sort(net.astro_input_sinks_.begin(), net.astro_input_sinks_.end());
+    return 0;
 }
 
 // ---- Free functions of the reference, exposed for known-answer checks ----

@@ -94,3 +94,36 @@ def test_drop_in_backend_pipelined_cell_ranges():
             assert np.array_equal(gpu.pull_calcium(), rCa), step
     gCa, gIP3, gh = gpu.destroy()
     assert np.array_equal(gCa, rCa) and np.array_equal(gIP3, rIP3) and np.array_equal(gh, rh)
+
+
+@pytest.mark.parametrize("uniform_params", [False, True])
+def test_drop_in_update_without_push_sees_zero_input(uniform_params):
+    """The reference kernel zeroes the input after each update, so an update
+    with no push before it sees zero input.  The engine reads the input only
+    after a push and never writes it; the results must still be the oracle's
+    for any mix of pushed and unpushed steps, with per-cell parameters that
+    differ or that are all equal (held as scalars)."""
+    rng = np.random.default_rng(9)
+    n = 1003
+    w = ScalingWorkload(n)
+    Ca, IP3, h = w.initial_state()
+    if uniform_params:
+        params = [np.full(n, v) for v in (w.Ca_tot, w.IP3_0, w.tau_IP3, w.delta_IP3)]
+    else:
+        params = [v * (1 + 0.05 * rng.standard_normal(n))
+                  for v in (w.Ca_tot, w.IP3_0, w.tau_IP3, w.delta_IP3)]
+    gpu = AstroBackend(Ca, IP3, h, *params)
+    rCa, rIP3, rh = Ca.copy(), IP3.copy(), h.copy()
+    lib = ref.ref()
+    zero = np.zeros(n)
+    for step in range(40):
+        pushed = step % 3 == 0 or step % 7 == 1
+        inp = np.where(rng.random(n) < 0.3, rng.random(n), 0.0) if pushed else zero
+        if pushed:
+            gpu.push_input(inp)
+        gpu.update(w.consts, w.h_step, 1)
+        lib.ref_astro_advance(ref._dp(w.consts), n, *[ref._dp(p) for p in params],
+                              ref._dp(inp), None, w.h_step, 1, ref._dp(rCa), ref._dp(rIP3),
+                              ref._dp(rh))
+    gCa, gIP3, gh = gpu.pull_state()
+    assert np.array_equal(gCa, rCa) and np.array_equal(gIP3, rIP3) and np.array_equal(gh, rh)
