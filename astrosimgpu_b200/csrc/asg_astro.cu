@@ -89,13 +89,12 @@ __device__ __forceinline__ void advance_cell(const StepArgs& a, const AstroArray
     } else {
         in = s.input[i];
     }
-    double noise = 0.0;
-    if (kNoise) {
-        noise = a.independent
-                    ? a.noise_std * normal_clamped(a.noise_seed, a.noise_index * kStreamStride +
-                                                                     static_cast<std::uint64_t>(a.i0 + i))
-                    : a.shared_noise;
-    }
+    // kNoise: independent per-cell draws; otherwise the step's shared value
+    // (0 with noise off, as the reference passes it).
+    const double noise =
+        kNoise ? a.noise_std * normal_clamped(a.noise_seed, a.noise_index * kStreamStride +
+                                                                static_cast<std::uint64_t>(a.i0 + i))
+               : a.shared_noise;
     if (kUniform) {
         astro_rk4(a.k, a.u.Ca_tot, a.u.IP3_0, a.u.tau, a.u.inv_tau, a.u.delta, in, noise, ca, ip3,
                   hh);
@@ -201,23 +200,47 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 template <bool kUniform, int kInput, bool kNoise>
 cudaError_t launch_astro(int shape, int sms, StepArgs a, AstroArrays s, cudaStream_t st) {
+    // Independent noise (log and cos per cell) is compiled for one shape: one
+    // cell per thread, 128 threads, 6 blocks per SM (85 registers, no spills).
+    if (kNoise) shape = 4;
     const Shape sh = kShapes[shape];
     const std::int64_t units = std::max<std::int64_t>(1, a.n / sh.cells);
     const std::int64_t want = (units + sh.block - 1) / sh.block;
     const std::int64_t cap = static_cast<std::int64_t>(sms) * sh.min_blocks * 4;
     const int grid = static_cast<int>(std::max<std::int64_t>(1, std::min(want, cap)));
-    switch (shape) {
-        case 0: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 4><<<grid, 128, 0, st>>>(a, s); break;
-        case 1: astro_step_kernel<kUniform, kInput, kNoise, 1, 128, 8><<<grid, 128, 0, st>>>(a, s); break;
-        case 2: astro_step_kernel<kUniform, kInput, kNoise, 1, 256, 4><<<grid, 256, 0, st>>>(a, s); break;
-        case 3: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 6><<<grid, 128, 0, st>>>(a, s); break;
-        case 4: astro_step_kernel<kUniform, kInput, kNoise, 1, 128, 6><<<grid, 128, 0, st>>>(a, s); break;
-        case 5: astro_step_kernel<kUniform, kInput, kNoise, 1, 64, 12><<<grid, 64, 0, st>>>(a, s); break;
-        case 6: astro_step_kernel<kUniform, kInput, kNoise, 4, 64, 8><<<grid, 64, 0, st>>>(a, s); break;
-        case 7: astro_step_kernel<kUniform, kInput, kNoise, 4, 128, 4><<<grid, 128, 0, st>>>(a, s); break;
-        default: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 5><<<grid, 128, 0, st>>>(a, s); break;
+    if constexpr (kNoise) {
+        astro_step_kernel<kUniform, kInput, kNoise, 1, 128, 6><<<grid, 128, 0, st>>>(a, s);
+    } else {
+        switch (shape) {
+            case 0: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 4><<<grid, 128, 0, st>>>(a, s); break;
+            case 1: astro_step_kernel<kUniform, kInput, kNoise, 1, 128, 8><<<grid, 128, 0, st>>>(a, s); break;
+            case 2: astro_step_kernel<kUniform, kInput, kNoise, 1, 256, 4><<<grid, 256, 0, st>>>(a, s); break;
+            case 3: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 6><<<grid, 128, 0, st>>>(a, s); break;
+            case 4: astro_step_kernel<kUniform, kInput, kNoise, 1, 128, 6><<<grid, 128, 0, st>>>(a, s); break;
+            case 5: astro_step_kernel<kUniform, kInput, kNoise, 1, 64, 12><<<grid, 64, 0, st>>>(a, s); break;
+            case 6: astro_step_kernel<kUniform, kInput, kNoise, 4, 64, 8><<<grid, 64, 0, st>>>(a, s); break;
+            case 7: astro_step_kernel<kUniform, kInput, kNoise, 4, 128, 4><<<grid, 128, 0, st>>>(a, s); break;
+            default: astro_step_kernel<kUniform, kInput, kNoise, 2, 128, 5><<<grid, 128, 0, st>>>(a, s); break;
+        }
     }
     return cudaGetLastError();
+}
+
+// The drop-in update's kernel for its parameter form, input and noise.
+template <bool kUniform>
+cudaError_t launch_update_p(bool pending, bool noisy, int shape, int sms, const StepArgs& a,
+                            const AstroArrays& s, cudaStream_t st) {
+    if (noisy)
+        return pending ? launch_astro<kUniform, kInputArray, true>(shape, sms, a, s, st)
+                       : launch_astro<kUniform, kInputNone, true>(shape, sms, a, s, st);
+    return pending ? launch_astro<kUniform, kInputArray, false>(shape, sms, a, s, st)
+                   : launch_astro<kUniform, kInputNone, false>(shape, sms, a, s, st);
+}
+
+cudaError_t launch_update(bool uniform, bool pending, bool noisy, int shape, int sms,
+                          const StepArgs& a, const AstroArrays& s, cudaStream_t st) {
+    return uniform ? launch_update_p<true>(pending, noisy, shape, sms, a, s, st)
+                   : launch_update_p<false>(pending, noisy, shape, sms, a, s, st);
 }
 
 __global__ void advance_counter_kernel(std::int64_t* base, std::int64_t by) { *base += by; }
@@ -410,9 +433,11 @@ int asg_astro_create(uint32_t n, const double* Ca, const double* IP3, const doub
         };
         e->params_uniform = same(Ca_tot) && same(IP3_0) && same(tau_IP3) && same(delta_IP3);
         if (e->params_uniform) {
-            if (!asg::divisor_ok(tau_IP3[0]))
+            if (!asg::divisor_ok(tau_IP3[0]) || !asg::diff_param_ok(Ca_tot[0]) ||
+                !asg::diff_param_ok(IP3_0[0]))
                 st = asg::fail(ASG_ERR_UNSUPPORTED,
-                               "asg_astro_create: tau_IP3 = %g outside [2^-46, 2^63]", tau_IP3[0]);
+                               "asg_astro_create: tau_IP3 outside [2^-46, 2^63] or Ca_tot / IP3_0 "
+                               "outside [2^-906, 2^976] in magnitude");
             e->up = asg::UniformParams{Ca_tot[0], IP3_0[0], tau_IP3[0], delta_IP3[0],
                                        1.0 / tau_IP3[0]};
             Ca_tot = IP3_0 = tau_IP3 = delta_IP3 = nullptr;  // nothing per cell to upload
@@ -428,6 +453,10 @@ int asg_astro_create(uint32_t n, const double* Ca, const double* IP3, const doub
                 st = asg::fail(ASG_ERR_UNSUPPORTED,
                                "asg_astro_create: tau_IP3[%u] = %g outside [2^-46, 2^63]", i,
                                tau_IP3[i]);
+            else if (!asg::diff_param_ok(Ca_tot[i]) || !asg::diff_param_ok(IP3_0[i]))
+                st = asg::fail(ASG_ERR_UNSUPPORTED,
+                               "asg_astro_create: Ca_tot[%u] or IP3_0[%u] has a magnitude outside "
+                               "[2^-906, 2^976]", i, i);
             inv[i] = 1.0 / tau_IP3[i];
         }
         upload(e->inv_tau, inv.data(), false);
@@ -559,19 +588,8 @@ int asg_astro_update(asg_astro* s, const double* consts, double h_step, int32_t 
         ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_out[c], 0));  // last Ca copy read it
         a.n = e->piece_end(c) - b;
         a.i0 = b;
-        const asg::AstroArrays arr = e->arrays_at(b);
-        cudaError_t le;
-        if (e->params_uniform)
-            le = pending ? asg::launch_astro<true, asg::kInputArray, true>(e->shape, e->sms, a, arr,
-                                                                          e->stream)
-                         : asg::launch_astro<true, asg::kInputNone, true>(e->shape, e->sms, a, arr,
-                                                                         e->stream);
-        else
-            le = pending ? asg::launch_astro<false, asg::kInputArray, true>(e->shape, e->sms, a,
-                                                                           arr, e->stream)
-                         : asg::launch_astro<false, asg::kInputNone, true>(e->shape, e->sms, a,
-                                                                          arr, e->stream);
-        ASG_CUDA(le);
+        ASG_CUDA(asg::launch_update(e->params_uniform, pending, a.independent != 0, e->shape,
+                                    e->sms, a, e->arrays_at(b), e->stream));
         ASG_CUDA(cudaEventRecord(e->ev_k[c], e->stream));
     }
     e->input_pending = false;
@@ -589,9 +607,11 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
         return asg::fail(ASG_ERR_ARG, "asg_astro_run_bernoulli: NULL argument");
     if (count < 0 || first < 0 || substeps < 0)
         return asg::fail(ASG_ERR_ARG, "asg_astro_run_bernoulli: negative step range");
-    if (!asg::divisor_ok(consts[9]) || (uniform && !asg::divisor_ok(tau_IP3)))
+    if (!asg::divisor_ok(consts[9]) ||
+        (uniform && (!asg::divisor_ok(tau_IP3) || !asg::diff_param_ok(Ca_tot) ||
+                     !asg::diff_param_ok(IP3_0))))
         return asg::fail(ASG_ERR_UNSUPPORTED, "asg_astro_run_bernoulli: ratio_ER_cyt or tau_IP3 "
-                         "outside [2^-46, 2^63]");
+                         "outside [2^-46, 2^63], or Ca_tot / IP3_0 outside [2^-906, 2^976]");
     auto* e = reinterpret_cast<AstroEngine*>(s);
     if (!uniform && !e->has_params)
         return asg::fail(ASG_ERR_STATE, "asg_astro_run_bernoulli: no per-cell parameters");
@@ -926,6 +946,8 @@ extern "C" int asg_astro_update_noalloc(uint32_t n, double* Ca, double* IP3, dou
     const asg::AstroArrays arr{Ca, IP3, h, ip3_input, Ca_tot, IP3_0, tau_IP3, inv_tau, delta_IP3};
     // Shape 1: one cell per thread with 8-byte accesses, so caller arrays need
     // no more than double alignment.
-    ASG_CUDA((asg::launch_astro<false, asg::kInputArrayZero, true>(1, sms, a, arr, st)));
+    ASG_CUDA(a.independent
+                 ? (asg::launch_astro<false, asg::kInputArrayZero, true>(1, sms, a, arr, st))
+                 : (asg::launch_astro<false, asg::kInputArrayZero, false>(1, sms, a, arr, st)));
     return ASG_OK;
 }

@@ -157,6 +157,32 @@ __host__ __device__ __forceinline__ double div_by(double a, double b, double y) 
 }
 
 
+// (x - y) / b through the reciprocal y_b = RN(1/b), without div_by's
+// exponent test, for a numerator formed from a model parameter: one of x, y
+// is a parameter of magnitude in [2^-906, 2^976] (checked on the host when
+// the parameters are set).  A non-zero x - y then has a magnitude of at least
+// 2^-959 -- if the other operand is below half the parameter the difference
+// exceeds 2^-907, else both exponents are >= -907 and the difference is a
+// multiple of 2^-959 -- so the remainder stays normal; x - y is never -0 (a
+// difference is -0 only for -0 - +0, and the parameter is non-zero) and +0
+// gives the IEEE +0; and the quotient is finite while |x - y| < 2^977, far
+// beyond any concentration or potential of the model.  Under those
+// conditions Markstein's theorem makes the result the IEEE (x - y) / b.
+// tests/div_by_check.cu checks it over every operand class it covers.
+__host__ __device__ __forceinline__ double div_diff_by(double x, double y, double b,
+                                                       double yb) {
+    const double a = x - y;
+    const double q = a * yb;
+    const double r = fma(-q, b, a);
+    return fma(r, yb, q);
+}
+
+// Magnitude range a parameter needs for div_diff_by (see there).
+__host__ __device__ __forceinline__ bool diff_param_ok(double p) {
+    const double m = p < 0.0 ? -p : p;
+    return m >= 0x1p-906 && m <= 0x1p976;
+}
+
 // ------------------------------------------------------ Li-Rinzel astrocyte
 
 // Population constants, with the run-time constant products of the
@@ -181,11 +207,13 @@ struct AstroRates {
 
 // d/dt of (Ca, IP3, h) for one cell.
 // `tau` and `inv_tau` (its correctly rounded reciprocal) give dIP3 with
-// div_by; the result is the IEEE quotient (IP3_0 - IP3) / tau.
+// div_diff_by; the result is the IEEE quotient (IP3_0 - IP3) / tau, as the ER
+// calcium is (Ca_tot - Ca) / ratio_ER_cyt, for Ca_tot and IP3_0 within
+// diff_param_ok (checked where the parameters enter the engine).
 __device__ __forceinline__ AstroRates li_rinzel(const AstroK& k, double ca_tot, double ip3_0,
                                                 double tau, double inv_tau, double ca, double ip3,
                                                 double hh, double noise) {
-    const double er = div_by(ca_tot - ca, k.ratio_ER_cyt, k.inv_ratio);  // ER calcium
+    const double er = div_diff_by(ca_tot, ca, k.ratio_ER_cyt, k.inv_ratio);  // ER calcium
     const double ip3_k1 = ip3 + k.Kd_IP3_1;
     const double m = ip3 / ip3_k1;                      // IP3 activation
     const double n = ca / (ca + k.Kd_act);              // Ca activation
@@ -201,7 +229,7 @@ __device__ __forceinline__ AstroRates li_rinzel(const AstroK& k, double ca_tot, 
     const double close_rate = k.k_IP3R * ca;
     AstroRates r;
     r.Ca = release - uptake + leak + noise;
-    r.IP3 = div_by(ip3_0 - ip3, tau, inv_tau);
+    r.IP3 = div_diff_by(ip3_0, ip3, tau, inv_tau);
     r.h = open_rate * (1.0 - hh) - close_rate * hh;
     return r;
 }

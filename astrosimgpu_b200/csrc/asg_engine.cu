@@ -533,6 +533,21 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
                 if (!divisor_ok(d.tau_IP3[a]))
                     return fail(ASG_ERR_UNSUPPORTED, "tau_IP3[%u] = %g outside [2^-46, 2^63]", a,
                                 d.tau_IP3[a]);
+        // Minuends of the astrocyte's divided differences (div_diff_by).
+        auto diff_check = [NA](const char* name, const double* arr, double u) {
+            if (NA == 0) return ASG_OK;
+            if (arr == nullptr)
+                return diff_param_ok(u) ? ASG_OK
+                                        : fail(ASG_ERR_UNSUPPORTED, "%s = %g: magnitude must be "
+                                               "in [2^-906, 2^976]", name, u);
+            for (std::uint32_t a = 0; a < NA; ++a)
+                if (!diff_param_ok(arr[a]))
+                    return fail(ASG_ERR_UNSUPPORTED, "%s[%u] = %g: magnitude must be in "
+                                "[2^-906, 2^976]", name, a, arr[a]);
+            return ASG_OK;
+        };
+        ASG_TRY(diff_check("Ca_tot", d.Ca_tot, d.Ca_tot_u));
+        ASG_TRY(diff_check("IP3_0", d.IP3_0, d.IP3_0_u));
     }
 
     auto inst = std::make_unique<Instance>();

@@ -180,7 +180,7 @@ class RefNetwork:
 
     def run(self, count: int, cap: int | None = None):
         """Advance `count` steps; returns (steps, sources) of the spikes."""
-        cap = cap if cap is not None else max(1024, self.n * count // 50 + 1024)
+        cap = cap if cap is not None else self.n * count + 1  # at most one spike per cell-step
         st = np.zeros(cap, np.int64)
         src = np.zeros(cap, np.uint32)
         total = int(ref().ref_net_run(self.h, self.step, count, st.ctypes.data_as(I64),

@@ -24,6 +24,10 @@
 //   hard        mantissas of all ones, powers of two and near-powers of two
 //   zero        a = +0 (and, separately, a = -0 in class neg_zero, whose IEEE
 //               quotient is -0)
+//   diff        div_diff_by(x, y, b, RN(1/b)) against IEEE (x - y) / b, where
+//               x or y is a parameter of magnitude in [2^-906, 2^976] and the
+//               other operand is anything finite: near-equal, equal, zero,
+//               subnormal, or of any magnitude (|x - y| < 2^977)
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -153,7 +157,42 @@ int main(int argc, char** argv) {
         negzero.check(-0.0, b);
     }
 
-    for (const Tally* t : {&random, &engine, &tiny, &subq, &huge, &hard, &zero, &negzero})
-        t->print();
+    // Divided differences with a parameter operand (div_diff_by).
+    struct DiffTally : Tally {
+        void check_diff(double x, double y, double b) {
+            const double want = (x - y) / b;
+            const double got = asg::div_diff_by(x, y, b, 1.0 / b);
+            ++cases;
+            if (bits(got) != bits(want)) {
+                if (bad < 3)
+                    std::fprintf(stderr, "%s: x=%a y=%a b=%a got=%a ieee=%a\n", name, x, y, b, got,
+                                 want);
+                ++bad;
+            }
+        }
+    } diff;
+    diff.name = "diff";
+    for (long long i = 0; i < n / 4; ++i) {
+        const double p = rng.value(-906, 975);
+        double other;
+        switch (rng.next() % 6) {
+            case 0: other = p * (1.0 + std::ldexp(2.0 * rng.unit() - 1.0, -(int)(rng.next() % 50))); break;
+            case 1: other = p; break;
+            case 2: other = (rng.next() & 1) ? 0.0 : -0.0; break;
+            case 3: other = from_bits(rng.next() & 0x800FFFFFFFFFFFFFULL); break;  // subnormal
+            case 4: other = rng.value(-1022, 975); break;
+            default: other = std::nextafter(p, (rng.next() & 1) ? 1e308 : -1e308); break;
+        }
+        double b = (rng.next() & 1) ? divisors[rng.next() % (sizeof divisors / sizeof divisors[0])]
+                                    : std::fabs(rng.value(-46, 62));
+        if (rng.next() & 1) b = -b;
+        const bool param_first = rng.next() & 1;
+        const double x = param_first ? p : other, y = param_first ? other : p;
+        if (std::fabs(x - y) >= 0x1p977) continue;
+        diff.check_diff(x, y, b);
+    }
+
+    const Tally* all[] = {&random, &engine, &tiny, &subq, &huge, &hard, &zero, &negzero, &diff};
+    for (const Tally* t : all) t->print();
     return 0;
 }

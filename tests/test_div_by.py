@@ -10,7 +10,10 @@ the magnitudes the model produces, and the cases the theorem excludes -- a
 numerator small enough for the remainder to be subnormal, subnormal
 quotients, quotients at the overflow threshold, mantissas of all ones and
 powers of two, and signed zeros.  Every class must match bit for bit: the
-excluded cases take the IEEE division itself."""
+excluded cases take the IEEE division itself.  div_diff_by, the astrocyte
+right-hand side's form without the exponent test, is checked the same way on
+differences with a parameter operand of magnitude in [2^-906, 2^976] (the
+range the engine enforces for Ca_tot and IP3_0) and any other operand."""
 import os
 import shutil
 import subprocess
@@ -43,7 +46,7 @@ def test_div_by_equals_ieee_division(checker, seed):
         name, cases, bad = line.split()
         rows[name] = (int(cases), int(bad))
     assert set(rows) == {"random", "engine", "tiny_a", "sub_q", "huge", "hard", "zero",
-                         "neg_zero"}
+                         "neg_zero", "diff"}
     for name, (cases, bad) in rows.items():
         assert cases > 0, name
         assert bad == 0, (name, cases, bad, out.stderr[:500])
