@@ -118,6 +118,14 @@ class AstroBackend:
         _lib.call("asg_astro_last_timing", self._h, C.byref(ms), C.byref(k))
         return ms.value, k.value
 
+    def last_timing(self):
+        """(device ms, kernels) of the last run_bernoulli call, or of every
+        update since the previous read (waits for them)."""
+        ms = C.c_double()
+        k = C.c_int64()
+        _lib.call("asg_astro_last_timing", self._h, C.byref(ms), C.byref(k))
+        return ms.value, k.value
+
     def set_shape(self, shape: int):
         """Use launch shape `shape` (raises AsgError outside the valid range)."""
         _lib.call("asg_astro_set_shape", self._h, int(shape))

@@ -355,7 +355,7 @@ struct AstroEngine {
     // Events keep each range's order: input copy -> update -> Ca copy, and
     // the next step's input copy and update after this step's update and Ca
     // copy of the same range.
-    static constexpr int kMaxPieces = 8;
+    static constexpr int kMaxPieces = 16;
     static constexpr std::int64_t kPieceCells = 1 << 18;
     cudaStream_t h2d = nullptr, d2h = nullptr;
     cudaEvent_t ev_in[kMaxPieces] = {}, ev_k[kMaxPieces] = {}, ev_out[kMaxPieces] = {};
@@ -582,19 +582,33 @@ int asg_astro_update(asg_astro* s, const double* consts, double h_step, int32_t 
     // 313-322); otherwise the caller's shared value (0) enters the RHS.
     if (!(noise_std > 0.0)) a.independent = 0;
     const bool pending = e->input_pending;
-    for (int c = 0; c < e->pieces(); ++c) {
-        const std::int64_t b = e->piece_begin(c);
-        ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_in[c], 0));   // this range's input
-        ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_out[c], 0));  // last Ca copy read it
-        a.n = e->piece_end(c) - b;
-        a.i0 = b;
-        ASG_CUDA(asg::launch_update(e->params_uniform, pending, a.independent != 0, e->shape,
-                                    e->sms, a, e->arrays_at(b), e->stream));
-        ASG_CUDA(cudaEventRecord(e->ev_k[c], e->stream));
+    if (!pending) {
+        // No input copy to overlap: one launch over every cell, after the
+        // last calcium copies of every range have read the state.
+        for (int c = 0; c < e->pieces(); ++c)
+            ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_out[c], 0));
+        a.n = e->n;
+        a.i0 = 0;
+        ASG_CUDA(asg::launch_update(e->params_uniform, false, a.independent != 0, e->shape,
+                                    e->sms, a, e->arrays(), e->stream));
+        for (int c = 0; c < e->pieces(); ++c)
+            ASG_CUDA(cudaEventRecord(e->ev_k[c], e->stream));
+        e->upd_calls += 1;
+    } else {
+        for (int c = 0; c < e->pieces(); ++c) {
+            const std::int64_t b = e->piece_begin(c);
+            ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_in[c], 0));   // this range's input
+            ASG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_out[c], 0));  // last Ca copy read it
+            a.n = e->piece_end(c) - b;
+            a.i0 = b;
+            ASG_CUDA(asg::launch_update(e->params_uniform, true, a.independent != 0, e->shape,
+                                        e->sms, a, e->arrays_at(b), e->stream));
+            ASG_CUDA(cudaEventRecord(e->ev_k[c], e->stream));
+        }
+        e->upd_calls += e->pieces();
     }
     e->input_pending = false;
     ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
-    e->upd_calls += e->pieces();
     return ASG_OK;
 }
 

@@ -245,6 +245,29 @@ class Batch:
                   C.byref(cnt))
         return st[:n], src[:n]
 
+    def fetch_record(self, inst: int):
+        """Recorded rows of instance `inst` since its last fetch (see
+        Network.fetch_record)."""
+        na_rows, nn_rows = C.c_int64(), C.c_int64()
+        _lib.call("asg_batch_fetch_record", self._h, inst, None, None, None, 0, C.byref(na_rows),
+                  None, None, None, 0, C.byref(nn_rows))
+        d = self.descs[inst]
+        n, na = d.n_exc + d.n_inh, d.n_astro
+        am, nm = min(self.rec.astro_max, na), min(self.rec.neuron_max, n)
+        a_st = np.zeros(max(na_rows.value, 1), np.int64)
+        ca = np.zeros(max(na_rows.value * am, 1))
+        ip3 = np.zeros(max(na_rows.value * am, 1))
+        n_st = np.zeros(max(nn_rows.value, 1), np.int64)
+        v = np.zeros(max(nn_rows.value * nm, 1))
+        isic = np.zeros(max(nn_rows.value * nm, 1))
+        _lib.call("asg_batch_fetch_record", self._h, inst, _lib.i64ptr(a_st), _lib.dptr(ca),
+                  _lib.dptr(ip3), na_rows.value, C.byref(na_rows), _lib.i64ptr(n_st),
+                  _lib.dptr(v), _lib.dptr(isic), nn_rows.value, C.byref(nn_rows))
+        ra, rn = na_rows.value, nn_rows.value
+        return dict(astro_steps=a_st[:ra], Ca=ca[:ra * am].reshape(ra, am),
+                    IP3=ip3[:ra * am].reshape(ra, am), neuron_steps=n_st[:rn],
+                    V=v[:rn * nm].reshape(rn, nm), I_sic=isic[:rn * nm].reshape(rn, nm))
+
     def state(self, inst: int):
         d = self.descs[inst]
         st, arrs = _alloc_state(d.n_exc + d.n_inh, d.n_astro)
@@ -339,3 +362,17 @@ class Server:
         except Exception:
             pass
 
+
+def calcium_analysis(times, ca, threshold, merge_gap, win_start, win_end, width, shift):
+    """Calcium analysis of traces (asg_calcium_analysis, the semantics of the
+    reference's analysis.cpp): `times` and `ca` are cells x samples.  Returns
+    active cells, transients, mean duration (ms), pairs correlated and the
+    mean pairwise correlation."""
+    t = np.ascontiguousarray(times, np.float64)
+    c = np.ascontiguousarray(ca, np.float64)
+    out = np.zeros(5)
+    _lib.call("asg_calcium_analysis", _lib.dptr(t), _lib.dptr(c), int(c.shape[0]),
+              int(c.shape[1]), float(threshold), float(merge_gap), float(win_start),
+              float(win_end), float(width), float(shift), _lib.dptr(out))
+    return dict(active=int(out[0]), transients=int(out[1]), mean_duration_ms=float(out[2]),
+                pairs=int(out[3]), correlation=float(out[4]))

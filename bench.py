@@ -14,14 +14,25 @@ noise off).  One "step" is one timestep of all N cells.
   asg_astro_pull_calcium), i.e. per step an 8N-byte host->device input copy
   and an 8N-byte device->host calcium copy from pinned host memory, exactly
   the movement pattern of the reference's published GPU numbers.
-- roofline: algorithmic HBM bytes of the step kernel (Ca, IP3, h read and
-  written: 48 B per cell-step) / measured launch time, against the measured
-  HBM copy bandwidth.
+- roofline: the binding one is the FP64 pipe (FP64 flops counted by ncu per
+  cell-step / launch time, against 148 SMs x 64 FP64 lanes x 2 flops x the
+  sampled SM clock); the HBM roofline (48 algorithmic bytes per cell-step
+  against the measured copy bandwidth) is reported beside it.
 - cpu_baseline: the reference's own astro_advance (built from its sources,
   oracle/_ref) over a bounded sample on the host cores with OpenMP.
 - reference_cuda_kernel: the reference's astro_update_kernel built for
-  sm_100a, timed on the same GPU (the GPU bar to beat).
-- network / batched / serving sub-objects: see --help.
+  sm_100a on the same GPU, and the same-contract A/B against it: the
+  drop-in asg_astro_update (per-cell parameter arrays, resident state,
+  back-to-back updates, no copies) on the calls the reference kernel is
+  timed on.
+- network_c0 / network_c2: the plain one-network path over the whole run of
+  use_case (20 s transient + 10 s) and paper_sparse at dt 0.05 ms (1 s),
+  each beside the reference CLI (OpenMP) timed on a bounded sample of the
+  same run on the host cores.
+- batched_c3: 64 instances of uneven size, 5 s each, batched vs one network
+  per launch.  serving_c4: a Poisson request stream (with one 1M-neuron /
+  1M-astrocyte request) through the continuous-batching server.
+  network_1m: that 1M network alone on the plain path.
 
 Multi-GPU: the astrocyte cells are independent, so N GPUs each run their
 own N-cell instance (weak scaling, no collective); rank 0 reports the sum.
@@ -32,9 +43,11 @@ import argparse
 import ctypes as C
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -43,8 +56,15 @@ sys.path.insert(0, ROOT)
 
 METRIC = "neuron-updates/s & HBM GB/s vs roofline; batched/served vs plain; p50/p99 lat"
 BYTES_PER_CELL_STEP = 48  # Ca, IP3, h: read + write, FP64
-# dram__bytes_read.sum + dram__bytes_write.sum of one astro_step_kernel launch,
-# from an ncu --set full capture of this workload (mean of two launches).
+# Per cell-step of astro_step_kernel<uniform, bernoulli> (substeps 1), from
+# an ncu capture of the headline workload (profiles/astro_step_kernel_N1e7.md):
+# FP64 thread instructions executed (DADD + DMUL + DFMA + the rest of the
+# FP64 pipe) and FP64 flops (DFMA counted twice).
+FP64_INST_PER_CELL_STEP = None
+FP64_FLOP_PER_CELL_STEP = None
+FP64_LANES_PER_SM = 64
+# dram__bytes_read.sum + dram__bytes_write.sum of one astro_step_kernel launch
+# at N = 1e7, from the same capture.
 NCU_TRAFFIC_PER_LAUNCH = {10_000_000: 420_363_392}
 
 
@@ -55,6 +75,15 @@ def load_peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def headline_config(cells, world):
+    """The workload both arms report (identical keys and values)."""
+    return {"workload": f"astrocyte kernel scaling, N={cells} cells per GPU, 1 step = 1 "
+                        "timestep (0.1 ms) of all cells, Bernoulli(0.01) IP3 input w=0.2, "
+                        "use_case astrocyte parameters, noise off, seed 1",
+            "cells": cells, "parallelism": f"replicas x{world}",
+            "l2": "working set 24 B/cell = 240 MB at N=1e7 > 126 MB L2 (no flush needed)"}
 
 
 class ClockSampler:
@@ -167,25 +196,28 @@ def pinned(n):
     """Pinned host float64 buffer as a numpy array (torch allocates it)."""
     import torch
     t = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    import numpy as np
-    arr = t.numpy()
-    return t, arr
+    return t, t.numpy()
+
+
+def sm_count():
+    import torch
+    return torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
 
 
 def bench_astro_scaling(args, rank, world, pg):
     import numpy as np
     import torch
 
-    from astrosimgpu_b200.astro import AstroBackend, ScalingWorkload
+    from astrosimgpu_b200 import _lib
+    from astrosimgpu_b200.astro import AstroBackend, ScalingWorkload, uniform_np
 
     n = args.cells
     w = ScalingWorkload(n, seed=1 + rank)
     Ca, IP3, h = w.initial_state()
     eng = AstroBackend(Ca, IP3, h)
-    shape, tuned_us = eng.autotune(w, steps=30)  # 9 shapes x 2 passes x 30 steps, ~0.13 s
-    # warm-up (untimed)
+    shape, tuned_us = eng.autotune(w, steps=30)  # 9 shapes x 2 passes x 30 steps, ~0.15 s
     step = 0
-    for _ in range(args.warmup):
+    for _ in range(args.warmup):  # untimed
         eng.run_bernoulli(w, step, 1)
         step += 1
     torch.cuda.synchronize()
@@ -199,6 +231,7 @@ def bench_astro_scaling(args, rank, world, pg):
     dev_ms = max_over_ranks(pg, dev_ms)
     per_launch_us = dev_ms * 1e3 / args.steps
     value = n * world * args.steps / (dev_ms * 1e-3)
+    clocks = clk.summary()
 
     # e2e through the drop-in ABI (per-cell parameter arrays, as the
     # reference backend holds them): H2D input + update + D2H Ca per step.
@@ -209,7 +242,6 @@ def bench_astro_scaling(args, rank, world, pg):
     ein_bufs = [pinned(n) for _ in range(2)]
     eca_t, eca = pinned(n)
     cells = np.arange(n, dtype=np.uint64)
-    from astrosimgpu_b200.astro import uniform_np
     for k, (_, buf) in enumerate(ein_bufs):
         u = uniform_np(w.seed, cells, 1000 + 10_000 + k)
         buf[:] = np.where(u < w.p, w.weight, 0.0)
@@ -220,12 +252,8 @@ def bench_astro_scaling(args, rank, world, pg):
         eca[:] = eng_e2e.pull_calcium()
     torch.cuda.synchronize()
     barrier(pg)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    ev0.record()
-    from astrosimgpu_b200 import _lib
     L = _lib.load()
     ein_ptrs = [_lib.dptr(buf) for _, buf in ein_bufs]
     for k in range(e2e_steps):
@@ -233,7 +261,6 @@ def bench_astro_scaling(args, rank, world, pg):
         _lib.check(L.asg_astro_update(eng_e2e._h, _lib.dptr(w.consts), w.h_step, w.substeps, 0.0,
                                       1, 0.0, 0, 0), "update")
         _lib.check(L.asg_astro_pull_calcium(eng_e2e._h, _lib.dptr(eca)), "pull")
-    ev1.record()
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     barrier(pg)
@@ -244,21 +271,35 @@ def bench_astro_scaling(args, rank, world, pg):
 
     peak, peak_kind = load_peaks()
     achieved = BYTES_PER_CELL_STEP * n / (per_launch_us * 1e-6) / 1e9
+    hbm = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "traffic": NCU_TRAFFIC_PER_LAUNCH.get(n),
+           "traffic_unit": "bytes per launch (ncu dram read + write)",
+           "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+           else peak_kind, "bytes_per_launch": BYTES_PER_CELL_STEP * n}
+    roofline = dict(hbm)
+    if FP64_FLOP_PER_CELL_STEP is not None and clocks.get("sm_mhz"):
+        sms = sm_count()
+        peak_tf = sms * FP64_LANES_PER_SM * 2 * clocks["sm_mhz"] * 1e6 / 1e12
+        ach_tf = FP64_FLOP_PER_CELL_STEP * n / (per_launch_us * 1e-6) / 1e12
+        inst_rate = FP64_INST_PER_CELL_STEP * n / (per_launch_us * 1e-6)
+        roofline = {"bound": "fp64", "achieved": ach_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                    "frac": ach_tf / peak_tf,
+                    "fp64_pipe_inst_frac": inst_rate / (sms * FP64_LANES_PER_SM *
+                                                        clocks["sm_mhz"] * 1e6),
+                    "flop_per_cell_step": FP64_FLOP_PER_CELL_STEP,
+                    "inst_per_cell_step": FP64_INST_PER_CELL_STEP,
+                    "peak_source": f"{sms} SMs x {FP64_LANES_PER_SM} FP64 lanes x 2 flops x "
+                                   "median sampled SM clock",
+                    "traffic": NCU_TRAFFIC_PER_LAUNCH.get(n),
+                    "hbm": hbm}
+    roofline["kernel"] = "astro_step_kernel<uniform,bernoulli>"
     out = {
         "value": value, "ms_per_step": dev_ms / args.steps, "kernels": kernels,
         "per_launch_us": per_launch_us,
         "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                 "steps": e2e_steps, "path": "asg_astro_push_input+update+pull_calcium"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak,
-                     "traffic": NCU_TRAFFIC_PER_LAUNCH.get(n),
-                     "traffic_unit": "bytes per launch (ncu dram read + write)",
-                     "peak_source": peak_kind,
-                     "bytes_per_launch": BYTES_PER_CELL_STEP * n,
-                     "kernel": "astro_step_kernel<uniform,bernoulli>"},
-        "clocks": clk.summary(),
-        "launch_shape": shape,
+        "roofline": roofline, "clocks": clocks, "launch_shape": shape,
     }
     return out, (w, Ca, IP3, h)
 
@@ -272,20 +313,15 @@ def network_bytes(n, na, astro_uniform, spike_edges, sic_edges, steps, sic_steps
         4 * sic_edges + (8 * na + 8 * n) * sic_steps
 
 
-def bench_network(name="paper_sparse_dt005", calls=20, steady_calls=5, **opts):
-    """Plain one-network path: the whole simulated time of a shipped config
-    (paper_sparse_dt005: 20,000 steps = 1 s), device time per call of 1,000
-    steps, with the algorithmic-byte roofline over the whole run and over
-    its last `steady_calls` calls (the SIC-active steady state)."""
+def run_network(m, uniform, calls, steady_calls=0, **opts):
+    """Whole run of model `m` on the plain path in `calls` equal calls;
+    device time per call, roofline over the run (and its last calls)."""
     from astrosimgpu_b200 import _lib
-    from astrosimgpu_b200.network import Model, Network, config_path
+    from astrosimgpu_b200.network import Network
     hbm, src = load_peaks()
-    t0 = time.perf_counter()
-    m = Model(config_path(name), pre_time=0.0)
-    build_s = time.perf_counter() - t0
     net = Network(m, record=_lib.RecordOpts(0, 10, 1, 0, 0), **opts)
-    per = max(1, m.sim_steps // calls)
-    uniform = not json.load(open(config_path(name))).get("randomize_astro", {}).get("enabled", False)
+    total = m.pre_steps + m.sim_steps
+    per = max(1, total // calls)
     rows = []
     prev = net.counters()
     kernels = 0
@@ -300,6 +336,7 @@ def bench_network(name="paper_sparse_dt005", calls=20, steady_calls=5, **opts):
         prev = c
     wall_s = time.perf_counter() - wall0
     n, na = net.n, net.na
+    net.close()
 
     def summary(sel):
         ms = sum(r[0] for r in sel)
@@ -314,18 +351,111 @@ def bench_network(name="paper_sparse_dt005", calls=20, steady_calls=5, **opts):
                 "synaptic_events_per_s": (se + sic) / (ms * 1e-3),
                 "roofline": {"bound": "hbm", "achieved": gb, "peak": hbm, "unit": "GB/s",
                              "frac": gb / hbm, "peak_source": src}}
-    full = summary(rows)
-    out = {"config": name, "neurons": n, "astrocytes": na, "dt_ms": m.dt, "build_s": build_s,
-           "kernels": kernels, "spikes": sum(r[3] for r in rows),
-           "wall_s_including_host": wall_s,
-           "per_1000_steps_us_per_step": [round(r[0] * 1e3 / per, 2) for r in rows],
+    out = {"neurons": n, "astrocytes": na, "dt_ms": m.dt, "kernels": kernels,
+           "spikes": sum(r[3] for r in rows), "wall_s_including_host": wall_s,
+           "per_call_us_per_step": [round(r[0] * 1e3 / per, 2) for r in rows],
            "engine_opts": opts}
-    out.update(full)
-    out["steady_state_last_%d_steps" % (per * steady_calls)] = summary(rows[-steady_calls:])
+    out.update(summary(rows))
+    if steady_calls:
+        out["steady_state_last_%d_steps" % (per * steady_calls)] = summary(rows[-steady_calls:])
+    return out, rows, per
+
+
+def reference_cli_sample(config_file, sim_ms, pre_ms, seed=1, timeout=600):
+    """The reference CLI (oracle/_ref/astrosimgpu, OpenMP on every host core,
+    OMP_PROC_BIND=spread) on `sim_ms` of recorded time after `pre_ms` of
+    transient; sim-s/wall-s from its own phase timers (run.txt's
+    real-time factor, recorded window only)."""
+    from oracle import ref
+    threads = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="spread")
+    with tempfile.TemporaryDirectory() as out:
+        t0 = time.perf_counter()
+        r = subprocess.run([ref.REF_CLI, "-c", config_file, "-o", out, "-t", str(sim_ms),
+                            "-p", str(pre_ms), "-s", str(seed), "--no-analysis"], env=env,
+                           capture_output=True, text=True, timeout=timeout)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr[-300:])
+        text = open(os.path.join(out, "run.txt")).read()
+    rtf = float(re.search(r"real-time factor\s+([0-9.eE+-]+)", text).group(1))
+    omp = int(re.search(r"OpenMP threads\s+(\d+)", text).group(1))
+    phases = {}
+    for key, label in (("input_gen", "background input"), ("update_astro", "update astrocytes"),
+                       ("update_neuron", "update neurons"), ("spike_cd", "spike delivery"),
+                       ("sic_gd", r"SIC gather\+deliver"), ("deliver", "arrival application")):
+        mm = re.search(label + r"\s+([0-9.]+)", text)
+        if mm:
+            phases[key] = float(mm.group(1))
+    return {"value": 1.0 / rtf, "unit": "sim-s/wall-s", "cores": omp, "kind": "reference",
+            "process_wall_s": wall, "phase_seconds": phases,
+            "sample": f"reference CLI (oracle/_ref/astrosimgpu, OpenMP {omp} threads, "
+                      f"OMP_PROC_BIND=spread): {sim_ms} ms recorded after {pre_ms} ms of "
+                      "transient, sim-s/wall-s from its run.txt real-time factor"}
+
+
+def bench_network_c0(cpu=True):
+    """use_case as shipped, the C0 throughput run: 20 s transient + 10 s."""
+    from astrosimgpu_b200.network import Model, config_path
+    m = Model(config_path("use_case"), sim_time=10000.0)
+    out, rows, per = run_network(m, uniform=False, calls=10)
+    out["config"] = "use_case, 20 s transient + 10 s recorded, dt 0.1 ms, seed 1"
+    if cpu:
+        try:
+            c = reference_cli_sample(config_path("use_case"), 2000.0, 0.0)
+            out["cpu_baseline"] = c
+            out["gpu_over_cpu_sim_s_per_wall_s"] = out["sim_s_per_wall_s"] / c["value"]
+        except Exception as e:  # noqa: BLE001
+            out["cpu_baseline"] = {"unavailable": str(e)[:200]}
     return out
 
 
-def bench_batched(sim_ms=500.0, n_inst=64, autotune=True):
+def bench_network_c2(cpu=True, **opts):
+    """paper_sparse at dt 0.05 ms, 1.5 ms delays: the whole 1 s (20,000
+    steps) in 20 calls, with the SIC-active steady state (last 5,000)."""
+    from astrosimgpu_b200.network import Model, config_path
+    name = "paper_sparse_dt005"
+    uniform = not json.load(open(config_path(name))).get("randomize_astro", {}).get("enabled",
+                                                                                      False)
+    t0 = time.perf_counter()
+    m = Model(config_path(name), pre_time=0.0)
+    build_s = time.perf_counter() - t0
+    out, rows, per = run_network(m, uniform=uniform, calls=20, steady_calls=5, **opts)
+    out["config"] = name + " (10k neurons, 10k astrocytes, ~10M synapses, dt 0.05 ms, 1 s)"
+    out["build_s"] = build_s
+    if cpu:
+        try:
+            sample_ms = 200.0
+            c = reference_cli_sample(config_path(name), sample_ms, 0.0)
+            c["sample"] += ("; the first 4,000 steps, before the SIC steady state (the "
+                            "reference's cheapest window)")
+            out["cpu_baseline"] = c
+            k = int(round(sample_ms / m.dt / per))
+            gpu_ms = sum(r[0] for r in rows[:k])
+            gpu_rate = (k * per * m.dt * 1e-3) / (gpu_ms * 1e-3)
+            out["gpu_sim_s_per_wall_s_same_window"] = gpu_rate
+            out["gpu_over_cpu_same_window"] = gpu_rate / c["value"]
+        except Exception as e:  # noqa: BLE001
+            out["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    return out
+
+
+def bench_network_1m():
+    """The largest serving request alone: 1M neurons, 1M astrocytes, fixed
+    in-degree 100 (device generator), 1,000 steps of 0.1 ms."""
+    from astrosimgpu_b200.network import Model
+    from astrosimgpu_b200.workloads import serving_config
+    t0 = time.perf_counter()
+    m = Model(text=serving_config(1_000_000, 99, 100.0), pre_time=0.0, fixed_indegree=100,
+              gen_device=0)
+    build_s = time.perf_counter() - t0
+    out, rows, per = run_network(m, uniform=False, calls=4)
+    out["config"] = "1M neurons / 1M astrocytes, fixed in-degree 100, use_case parameters, 100 ms"
+    out["build_s"] = build_s
+    return out
+
+
+def bench_batched(sim_ms=5000.0, n_inst=64, autotune=True):
     """64-instance sweep: batched engine vs one network per launch."""
     from astrosimgpu_b200 import _lib
     from astrosimgpu_b200.network import Batch, Model, Network
@@ -335,9 +465,8 @@ def bench_batched(sim_ms=500.0, n_inst=64, autotune=True):
     steps = models[0].sim_steps
     dt = models[0].dt
     rec = _lib.RecordOpts(0, 10, 1, 0, 0)
-    # plain path: each instance on its own, one after another
     plain_ms, plain_kernels = 0.0, 0
-    for m in models:
+    for m in models:  # plain path: each instance on its own, one after another
         net = Network(m, record=rec, chunk_steps=64)
         net.step(64)  # warm (graph capture)
         net.step(steps)
@@ -353,6 +482,7 @@ def bench_batched(sim_ms=500.0, n_inst=64, autotune=True):
     sim_s = n_inst * steps * dt * 1e-3
     spikes = sum(b.counters(i)["spikes"] for i in range(n_inst))
     neurons = sum(mm.desc().n_exc + mm.desc().n_inh for mm in models)
+    b.close()
     return {"instances": n_inst, "steps": steps, "sim_ms_each": steps * dt,
             "total_neurons": neurons,
             "batched_ms": bms, "plain_ms": plain_ms,
@@ -363,7 +493,7 @@ def bench_batched(sim_ms=500.0, n_inst=64, autotune=True):
             "spikes": spikes}
 
 
-def bench_serving(n_req=30, rate_hz=20.0, big=False, **opts):
+def bench_serving(n_req=100, rate_hz=20.0, big=True, **opts):
     """Poisson request stream through the continuous-batching server."""
     import numpy as np
     from astrosimgpu_b200.network import Model, Server
@@ -386,46 +516,68 @@ def bench_serving(n_req=30, rate_hz=20.0, big=False, **opts):
     st = srv.stats()
     srv.close()
     lat = np.array([r.submit_to_done_ms for r in res])
+    adm = np.array([r.submit_to_admit_ms for r in res])
     events = sum(r.spike_edges + r.sic_edges for r in res)
     sim_s = sum(dur for (_, _, dur, _) in stream) * 1e-3
     neuron_steps = sum(n * m.sim_steps for (_, n, _, _), m in zip(stream, models))
     return {"requests": len(res), "arrival_rate_hz": rate_hz,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "admit_p50_ms": float(np.percentile(adm, 50)),
+            "admit_p99_ms": float(np.percentile(adm, 99)),
             "wall_s": wall, "synaptic_events_per_s": events / wall,
             "sim_s_per_wall_s": sim_s / wall, "neuron_updates_per_s": neuron_steps / wall,
+            "gpu_busy_frac": st["device_ms"] * 1e-3 / wall,
             "peak_resident": st["peak_resident"], "kernels": st["kernels"],
             "device_ms": st["device_ms"], "build_s": build_s,
+            "largest_request_neurons": max(int(n) for (_, n, _, _) in stream),
             "sizes": [int(n) for (_, n, _, _) in stream],
             "statuses": sorted(set(int(r.status) for r in res))}
 
 
 def reference_cuda_kernel(w, Ca, IP3, h, steps):
-    """The reference's astro_update_kernel (sm_100a build) on the same GPU."""
+    """The reference's astro_update_kernel (sm_100a build) on the same GPU,
+    and the drop-in asg_astro_update on the same contract: per-cell
+    parameter arrays given at create, resident state, `steps` back-to-back
+    updates with no push in between (the calls refcu_time_updates makes),
+    device-timed on each side.  Once with the C1 parameters (equal in every
+    cell) and once with per-cell parameters spread +-5 %."""
     import numpy as np
 
+    from astrosimgpu_b200.astro import AstroBackend
     from oracle import ref
     lib = ref.refcu()
     n = len(Ca)
-    Ca_tot = np.full(n, w.Ca_tot)
-    IP3_0 = np.full(n, w.IP3_0)
-    tau = np.full(n, w.tau_IP3)
-    delta = np.full(n, w.delta_IP3)
-    arrs = [np.ascontiguousarray(a) for a in (Ca, IP3, h, Ca_tot, IP3_0, tau, delta)]
-    s = lib.refcu_create(n, *[ref._dp(a) for a in arrs])
-    lib.refcu_time_updates(s, ref._dp(w.consts), w.h_step, w.substeps, 3)
-    ms = lib.refcu_time_updates(s, ref._dp(w.consts), w.h_step, w.substeps, steps)
+    rng = np.random.default_rng(3)
+    sets = {"uniform_values": [np.full(n, v) for v in (w.Ca_tot, w.IP3_0, w.tau_IP3,
+                                                       w.delta_IP3)],
+            "per_cell_values": [v * (1 + 0.05 * rng.standard_normal(n))
+                                for v in (w.Ca_tot, w.IP3_0, w.tau_IP3, w.delta_IP3)]}
+    out = {"steps": steps, "note": "reference astro_update_kernel, block 128, built -arch "
+                                   "sm_100a, resident state, no copies; ours asg_astro_update"}
     o = [np.empty(n) for _ in range(3)]
-    lib.refcu_destroy(s, *[ref._dp(a) for a in o])
-    us = ms * 1e3 / steps
-    return {"us_per_step": us, "cell_updates_per_s": n / (us * 1e-6), "steps": steps,
-            "note": "reference astro_update_kernel, block 128, built -arch sm_100a, "
-                    "resident state, no copies"}
+    for label, params in sets.items():
+        arrs = [np.ascontiguousarray(a) for a in (Ca, IP3, h, *params)]
+        s = lib.refcu_create(n, *[ref._dp(a) for a in arrs])
+        lib.refcu_time_updates(s, ref._dp(w.consts), w.h_step, w.substeps, 3)
+        ref_ms = lib.refcu_time_updates(s, ref._dp(w.consts), w.h_step, w.substeps, steps)
+        lib.refcu_destroy(s, *[ref._dp(a) for a in o])
+        eng = AstroBackend(Ca, IP3, h, *params)
+        eng.autotune(w, steps=20)
+        for rep in range(2):  # first pass warms up
+            for _ in range(steps):
+                eng.update(w.consts, w.h_step, w.substeps)
+            ms, _ = eng.last_timing()
+        eng.destroy()
+        ref_us, us = ref_ms * 1e3 / steps, ms * 1e3 / steps
+        out[label] = {"reference_us_per_step": ref_us, "asg_astro_update_us_per_step": us,
+                      "speedup": ref_us / us, "cell_updates_per_s": n / (us * 1e-6)}
+    out["us_per_step"] = out["uniform_values"]["reference_us_per_step"]
+    out["cell_updates_per_s"] = n / (out["us_per_step"] * 1e-6)
+    return out
 
 
 def cpu_baseline(w, budget_s=12.0):
     """Reference astro_advance on the host cores (OpenMP), bounded sample."""
-    import numpy as np
-
     from oracle import ref
     lib = ref.ref()
     threads = os.cpu_count() or 1
@@ -436,7 +588,6 @@ def cpu_baseline(w, budget_s=12.0):
     while secs < budget_s and steps < 1000:
         secs += ref.ref_astro_scaling(w, Ca, IP3, h, 1 + steps, 1, threads=threads)
         steps += 1
-    del np
     return {"value": n * steps / secs, "unit": "cell-updates/s", "cores": threads,
             "kind": "reference",
             "sample": f"{steps} steps x {n} cells of the same workload through the reference's "
@@ -465,9 +616,7 @@ def run_reference_arm(args, rank, world, pg):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"astrocyte kernel scaling, N={args.cells}, 1 step = 1 timestep "
-                               "(0.1 ms) of all cells, Bernoulli(0.01) IP3 input w=0.2",
-                   "cells": args.cells},
+        "config": headline_config(args.cells, world),
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads,
                          "kind": "reference",
                          "sample": f"{args.steps} full steps of {args.cells} cells through the "
@@ -477,6 +626,9 @@ def run_reference_arm(args, rank, world, pg):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+SUBS = ("network_c0", "network_c2", "batched_c3", "serving_c4", "network_1m")
 
 
 def main():
@@ -491,12 +643,11 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the reference CUDA kernel and sub-benchmarks")
     ap.add_argument("--skip", default="", help="comma list of sub-benchmarks to skip: "
-                    "network_c2,batched_c3,serving_c4")
+                    + ",".join(SUBS))
     ap.add_argument("--engine-mode", type=int, default=1,
                     help="network engine launches (--only network_c2): 1 graphs of per-step "
                          "kernels, 2 persistent chunk kernel")
-    ap.add_argument("--only", default="", choices=["", "astro", "network_c2", "batched_c3",
-                                                   "serving_c4"],
+    ap.add_argument("--only", default="", choices=("", "astro") + SUBS,
                     help="run one part alone and print its JSON (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -511,14 +662,20 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    subs = {"network_c0": lambda: bench_network_c0(cpu=not args.no_cpu_baseline),
+            "network_c2": lambda: bench_network_c2(cpu=not args.no_cpu_baseline),
+            "batched_c3": bench_batched, "serving_c4": bench_serving,
+            "network_1m": bench_network_1m}
     if args.only and args.only != "astro":
-        fn = {"network_c2": lambda: bench_network(use_graphs=max(args.engine_mode, 1)),
-              "batched_c3": bench_batched, "serving_c4": bench_serving}[args.only]
+        fn = subs[args.only]
+        if args.only == "network_c2":
+            fn = lambda: bench_network_c2(cpu=False, use_graphs=max(args.engine_mode, 1))  # noqa
         print(json.dumps({args.only: fn()}), flush=True)
         return 0
     res, (w, Ca, IP3, h) = bench_astro_scaling(args, rank, world, pg)
     if args.only == "astro":
-        print(json.dumps({"astro": {k: res[k] for k in ("value", "per_launch_us", "roofline", "e2e")}}))
+        print(json.dumps({"astro": {k: res[k] for k in ("value", "per_launch_us", "roofline",
+                                                        "e2e", "clocks")}}))
         return 0
 
     extras = {}
@@ -528,12 +685,11 @@ def main():
                                                                     min(args.steps, 50))
         except Exception as e:  # noqa: BLE001
             extras["reference_cuda_kernel"] = {"unavailable": str(e)[:200]}
-        for key, fn in (("network_c2", bench_network), ("batched_c3", bench_batched),
-                        ("serving_c4", bench_serving)):
+        for key in SUBS:
             if key in args.skip:
                 continue
             try:
-                extras[key] = fn()
+                extras[key] = subs[key]()
             except Exception as e:  # noqa: BLE001
                 extras[key] = {"unavailable": f"{type(e).__name__}: {str(e)[:300]}"}
     cpu = None
@@ -546,11 +702,7 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"astrocyte kernel scaling, N={args.cells} per GPU, 1 step = "
-                                   "1 timestep (0.1 ms) of all cells, Bernoulli(0.01) IP3 input "
-                                   "w=0.2, use_case astrocyte parameters, noise off",
-                       "cells_per_gpu": args.cells, "parallelism": f"replicas x{world}",
-                       "l2": "working set 24 B/cell = 240 MB > 126 MB L2 (no flush needed)"},
+            "config": headline_config(args.cells, world),
             "e2e": res["e2e"], "gpu_launches": res["kernels"], "roofline": res["roofline"],
             "clocks": res["clocks"], "per_launch_us": res["per_launch_us"],
             "launch_shape": res["launch_shape"],
