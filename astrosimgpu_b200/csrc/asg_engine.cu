@@ -473,10 +473,29 @@ int Engine::footprint(const asg_network_desc& d, int chunk_steps, std::uint64_t*
 
 int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int64_t first,
                 std::int64_t end, bool keep_spikes, int* id_out) {
-    // The chunks in flight keep running while the tables are prepared and
-    // uploaded (on the upload stream, into a new arena); they are collected
-    // only before the instance list changes, since they report statistics by
-    // instance position.
+    std::unique_ptr<Instance> inst;
+    ASG_TRY(prepare(d, rec, first, end, keep_spikes, true, &inst));
+    return commit(std::move(inst), id_out);
+}
+
+int Engine::commit(std::unique_ptr<Instance> inst, int* id_out) {
+    // The chunks in flight are collected before the instance list changes,
+    // since they report statistics by instance position.
+    ASG_TRY(finish_pending());
+    inst->id = next_id++;
+    resident_bytes += inst->arena_bytes;
+    *id_out = inst->id;
+    insts.push_back(std::move(inst));
+    dirty = true;
+    return ASG_OK;
+}
+
+int Engine::prepare(const asg_network_desc& d, const asg_record_opts* rec, std::int64_t first,
+                    std::int64_t end, bool keep_spikes, bool check_budget,
+                    std::unique_ptr<Instance>* out) {
+    // Touches no state the chunks in flight use: the tables are prepared and
+    // uploaded on the upload stream into a new arena, so a serving loop can
+    // run this on another thread while the engine's stream keeps stepping.
     const std::uint32_t NE = d.n_exc, NI = d.n_inh, N = NE + NI, NA = d.n_astro;
     if (d.dt <= 0.0) return fail(ASG_ERR_ARG, "dt must be positive");
     if (d.substeps < 1) return fail(ASG_ERR_ARG, "substeps must be at least 1");
@@ -750,7 +769,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
 
     std::size_t total = 0;
     for (const Seg& s : segs) total += align256(std::max<std::size_t>(s.bytes, 1));
-    if (resident_bytes + total > cfg.mem_budget)
+    if (check_budget && resident_bytes + total > cfg.mem_budget)
         return fail(ASG_ERR_OOM, "instance needs %zu device bytes; %llu of %llu in use", total,
                     static_cast<unsigned long long>(resident_bytes),
                     static_cast<unsigned long long>(cfg.mem_budget));
@@ -807,12 +826,7 @@ int Engine::add(const asg_network_desc& d, const asg_record_opts* rec, std::int6
     D.spike_log_cap = D.rec_spikes ? I.log_cap : 0;
     I.step = first;
     I.end = end;
-    ASG_TRY(finish_pending());
-    I.id = next_id++;
-    resident_bytes += total;
-    *id_out = I.id;
-    insts.push_back(std::move(inst));
-    dirty = true;
+    *out = std::move(inst);
     return ASG_OK;
 }
 

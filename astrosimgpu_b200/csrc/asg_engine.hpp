@@ -71,8 +71,19 @@ public:
     int init();
 
     // Adds an instance from a descriptor; it runs steps [first, end).
+    // add = prepare + commit.
     int add(const asg_network_desc& d, const asg_record_opts* rec, std::int64_t first,
             std::int64_t end, bool keep_spikes, int* id);
+    // Validates the descriptor, builds the instance's tables and uploads its
+    // arena on the upload stream.  Uses nothing the chunks in flight use, so
+    // it may run on another host thread while run_chunk steps (one prepare
+    // at a time).  check_budget: refuse beyond cfg.mem_budget (a caller that
+    // accounts for memory itself passes false).
+    int prepare(const asg_network_desc& d, const asg_record_opts* rec, std::int64_t first,
+                std::int64_t end, bool keep_spikes, bool check_budget,
+                std::unique_ptr<Instance>* out);
+    // Joins a prepared instance at this chunk boundary (same thread as run).
+    int commit(std::unique_ptr<Instance> inst, int* id);
     int remove(int id);
     Instance* find(int id);
     // Bytes an instance of this descriptor would hold on the device.

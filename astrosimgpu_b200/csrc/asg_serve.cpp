@@ -1,13 +1,15 @@
 // Serving: continuous batching of simulation requests over one Engine, and
 // the launch-shape autotuner of the batched sweep.
 //
-// A host thread owns the engine.  Each turn it (1) admits queued requests in
-// arrival order while their device footprint fits the budget and the
-// resident count allows, (2) removes cancelled ones, (3) runs one chunk of
-// steps for every resident request, and (4) retires requests that reached
-// their last step, recording submit->admit and submit->done latency.
-// Requests join and leave only at chunk boundaries, so a request's arithmetic
-// is the same alone and in any mix.
+// Two host threads share the engine.  The admission thread prepares queued
+// requests in arrival order while their device footprint fits the budget
+// (validation, device in-edge numbering, arena upload: everything that does
+// not touch the running batch) and stages them.  The stepping thread, at
+// each chunk boundary, joins the staged requests, removes cancelled ones,
+// runs one chunk of steps for every resident request, and retires requests
+// that reached their last step, recording submit->admit and submit->done
+// latency.  Requests join and leave only at chunk boundaries, so a request's
+// arithmetic is the same alone and in any mix.
 
 #include <algorithm>
 #include <chrono>
@@ -88,7 +90,7 @@ struct DescCopy {
     }
 };
 
-enum class ReqState { Queued, Running, Done };
+enum class ReqState { Queued, Preparing, Staged, Running, Done };
 
 struct Request {
     std::int64_t id = 0;
@@ -102,6 +104,8 @@ struct Request {
     Clock::time_point t_submit, t_admit, t_done;
     asg_request_result result{};
     std::vector<SpikeRec> spikes;
+    std::unique_ptr<Instance> prepared;  // built by the admission thread, not yet joined
+    std::string error;                   // text of a failed admission
 };
 
 }  // namespace
@@ -111,23 +115,30 @@ struct Server {
     std::uint64_t budget = 0;
     int max_instances = 256;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
-    std::deque<std::int64_t> queue;
+    // cv_work wakes the stepping loop (staged requests, cancels, stop);
+    // cv_admit the admission thread (submits, retirements, cancels, stop).
+    std::condition_variable cv_work, cv_admit, cv_done;
+    std::deque<std::int64_t> queue;   // submitted, waiting for admission
+    std::deque<std::int64_t> staged;  // prepared, waiting for a chunk boundary
     std::map<std::int64_t, std::unique_ptr<Request>> reqs;
     std::int64_t next_id = 1;
     bool stop = false;
     int loop_status = ASG_OK;
     std::string loop_error;
     std::int32_t resident = 0, peak_resident = 0;
-    std::uint64_t resident_bytes = 0;
-    std::thread thread;
+    std::int32_t in_admission = 0;       // preparing or staged
+    std::uint64_t resident_bytes = 0;    // footprints of running requests
+    std::uint64_t reserved_bytes = 0;    // footprints of requests in admission
+    std::int64_t retirements = 0;        // bumps whenever device memory frees up
+    std::thread thread, admit_thread;
 
     void loop();
+    void admit_loop();
     void retire(Request& r, int status);
 };
 
 void Server::retire(Request& r, int status) {
-    Instance* I = eng->find(r.inst);
+    Instance* I = r.inst >= 0 ? eng->find(r.inst) : nullptr;
     r.t_done = Clock::now();
     r.result.status = status;
     if (I != nullptr) {
@@ -143,53 +154,143 @@ void Server::retire(Request& r, int status) {
         resident_bytes -= r.footprint;
         eng->remove(r.inst);
         --resident;
+        ++retirements;
+        cv_admit.notify_all();
     }
-    r.result.submit_to_admit_ms =
-        r.state == ReqState::Queued ? ms_between(r.t_submit, r.t_done) : ms_between(r.t_submit, r.t_admit);
+    r.result.submit_to_admit_ms = r.state == ReqState::Running
+                                      ? ms_between(r.t_submit, r.t_admit)
+                                      : ms_between(r.t_submit, r.t_done);
     r.result.submit_to_done_ms = ms_between(r.t_submit, r.t_done);
     r.state = ReqState::Done;
     r.desc.reset();  // host copy no longer needed
+    r.prepared.reset();
 }
 
+// Admission, off the stepping loop: takes queued requests in arrival order
+// while their footprint fits the budget beside the resident and staged ones,
+// and prepares each (validation, in-edge numbering on the GPU, SIC lists,
+// arena upload) without holding the server lock, while the loop keeps
+// stepping the resident requests.  Prepared requests are staged; the loop
+// joins them at its next chunk boundary.
+void Server::admit_loop() {
+    std::unique_lock<std::mutex> lk(mu);
+    while (!stop) {
+        if (queue.empty()) {
+            cv_admit.wait(lk, [&] { return stop || !queue.empty(); });
+            continue;
+        }
+        Request& r = *reqs[queue.front()];
+        if (r.cancel) {
+            queue.pop_front();
+            retire(r, ASG_ERR_CANCELLED);
+            cv_done.notify_all();
+            continue;
+        }
+        if (resident + in_admission >= max_instances ||
+            resident_bytes + reserved_bytes + r.footprint > budget) {
+            const std::int64_t seen = retirements;
+            cv_admit.wait(lk, [&] { return stop || retirements != seen || r.cancel; });
+            continue;
+        }
+        queue.pop_front();
+        r.state = ReqState::Preparing;
+        reserved_bytes += r.footprint;
+        ++in_admission;
+        const std::int64_t seen = retirements;
+        const asg_network_desc* d = &r.desc->d;
+        lk.unlock();
+        asg_record_opts ro{};
+        ro.record_every = 1;
+        ro.spikes = r.keep_spikes ? 1 : 0;
+        std::unique_ptr<Instance> inst;
+        const int st = eng->prepare(*d, &ro, 0, r.n_steps, r.keep_spikes, false, &inst);
+        const std::string err = st != ASG_OK ? asg_last_error() : std::string();
+        lk.lock();
+        if (stop) {  // the server is shutting down or the loop failed
+            inst.reset();
+            reserved_bytes -= r.footprint;
+            --in_admission;
+            retire(r, loop_status != ASG_OK ? loop_status : ASG_ERR_CANCELLED);
+            cv_done.notify_all();
+            break;
+        }
+        if (st == ASG_ERR_OOM && (resident > 0 || in_admission > 1)) {
+            // the device is short of memory now: retry once something leaves
+            inst.reset();
+            reserved_bytes -= r.footprint;
+            --in_admission;
+            r.state = ReqState::Queued;
+            queue.push_front(r.id);
+            cv_admit.wait(lk, [&] { return stop || retirements != seen || r.cancel; });
+            continue;
+        }
+        if (st != ASG_OK) {
+            reserved_bytes -= r.footprint;
+            --in_admission;
+            r.error = err;
+            retire(r, st);
+            cv_done.notify_all();
+            continue;
+        }
+        r.prepared = std::move(inst);
+        r.state = ReqState::Staged;
+        staged.push_back(r.id);
+        cv_work.notify_one();
+    }
+}
+
+// Stepping: at each chunk boundary retire cancelled requests and join the
+// staged ones, run one chunk of steps for every resident request, and retire
+// those that reached their last step.  Requests join and leave only at chunk
+// boundaries, so a request's arithmetic is the same alone and in any mix.
 void Server::loop() {
     std::unique_lock<std::mutex> lk(mu);
     while (!stop) {
-        // cancellations and admissions at this step boundary
         for (auto& kv : reqs) {
             Request& r = *kv.second;
             if (r.cancel && r.state == ReqState::Running) retire(r, ASG_ERR_CANCELLED);
         }
-        while (!queue.empty()) {
-            Request& r = *reqs[queue.front()];
+        std::vector<Request*> joining;
+        while (!staged.empty()) {
+            Request& r = *reqs[staged.front()];
+            staged.pop_front();
+            reserved_bytes -= r.footprint;
+            --in_admission;
             if (r.cancel) {
-                queue.pop_front();
                 retire(r, ASG_ERR_CANCELLED);
                 continue;
             }
-            if (resident >= max_instances || resident_bytes + r.footprint > budget) break;
-            int id = -1;
-            asg_record_opts ro{};
-            ro.record_every = 1;
-            ro.spikes = r.keep_spikes ? 1 : 0;
-            const int st = eng->add(r.desc->d, &ro, 0, r.n_steps, r.keep_spikes, &id);
-            if (st == ASG_ERR_OOM && resident > 0) break;  // wait for memory to free up
-            queue.pop_front();
-            if (st != ASG_OK) {
-                r.state = ReqState::Done;
-                r.result.status = st;
-                r.t_done = Clock::now();
-                r.result.submit_to_done_ms = ms_between(r.t_submit, r.t_done);
-                continue;
+            joining.push_back(&r);
+        }
+        if (!joining.empty()) {
+            // the join waits for the chunks in flight: outside the lock
+            std::vector<int> ids(joining.size(), -1), sts(joining.size(), ASG_OK);
+            std::vector<std::string> errs(joining.size());
+            std::vector<std::unique_ptr<Instance>> prepared;
+            for (Request* r : joining) prepared.push_back(std::move(r->prepared));
+            lk.unlock();
+            for (std::size_t k = 0; k < joining.size(); ++k) {
+                sts[k] = eng->commit(std::move(prepared[k]), &ids[k]);
+                if (sts[k] != ASG_OK) errs[k] = asg_last_error();
             }
-            r.inst = id;
-            r.state = ReqState::Running;
-            r.t_admit = Clock::now();
-            resident_bytes += r.footprint;
-            peak_resident = std::max(peak_resident, ++resident);
+            lk.lock();
+            for (std::size_t k = 0; k < joining.size(); ++k) {
+                Request& r = *joining[k];
+                if (sts[k] != ASG_OK) {
+                    r.error = errs[k];
+                    retire(r, sts[k]);
+                    continue;
+                }
+                r.inst = ids[k];
+                r.state = ReqState::Running;
+                r.t_admit = Clock::now();
+                resident_bytes += r.footprint;
+                peak_resident = std::max(peak_resident, ++resident);
+            }
         }
         cv_done.notify_all();
         if (resident == 0) {
-            cv_work.wait(lk, [&] { return stop || !queue.empty(); });
+            cv_work.wait(lk, [&] { return stop || !staged.empty(); });
             continue;
         }
         // one chunk for every resident request, outside the lock
@@ -203,9 +304,15 @@ void Server::loop() {
         if (st != ASG_OK) {
             loop_status = st;
             loop_error = asg_last_error();
+            // every request not being prepared right now ends with the error
+            // (the admission thread ends the one it is preparing)
             for (auto& kv : reqs)
-                if (kv.second->state != ReqState::Done) retire(*kv.second, st);
+                if (kv.second->state != ReqState::Done && kv.second->state != ReqState::Preparing)
+                    retire(*kv.second, st);
+            queue.clear();
+            staged.clear();
             stop = true;
+            cv_admit.notify_all();
             break;
         }
         for (auto& kv : reqs) {
@@ -244,6 +351,7 @@ int asg_serve_create(const asg_serve_opts* opts, asg_server** out) {
     if (opts != nullptr && opts->max_instances > 0) s->max_instances = opts->max_instances;
     Server* raw = s.get();
     s->thread = std::thread([raw] { raw->loop(); });
+    s->admit_thread = std::thread([raw] { raw->admit_loop(); });
     *out = reinterpret_cast<asg_server*>(s.release());
     return ASG_OK;
 }
@@ -275,7 +383,7 @@ int asg_serve_submit(asg_server* sp, const asg_network_desc* desc, int64_t n_ste
         s->queue.push_back(r->id);
         s->reqs[r->id] = std::move(r);
     }
-    s->cv_work.notify_one();
+    s->cv_admit.notify_all();
     return ASG_OK;
 }
 
@@ -311,7 +419,7 @@ int asg_serve_wait(asg_server* sp, int64_t id, double timeout_ms, asg_request_re
     return r->result.status == ASG_OK || r->result.status == ASG_ERR_CANCELLED
                ? ASG_OK
                : asg::fail(r->result.status, "request %lld failed: %s", (long long)id,
-                           s->loop_error.c_str());
+                           r->error.empty() ? s->loop_error.c_str() : r->error.c_str());
 }
 
 int asg_serve_fetch_spikes(asg_server* sp, int64_t id, int64_t* steps, uint32_t* sources,
@@ -348,6 +456,7 @@ int asg_serve_cancel(asg_server* sp, int64_t id) {
         it->second->cancel = true;
     }
     s->cv_work.notify_one();
+    s->cv_admit.notify_all();
     return ASG_OK;
 }
 
@@ -374,6 +483,8 @@ int asg_serve_destroy(asg_server* sp) {
         s->stop = true;
     }
     s->cv_work.notify_all();
+    s->cv_admit.notify_all();
+    if (s->admit_thread.joinable()) s->admit_thread.join();
     if (s->thread.joinable()) s->thread.join();
     delete s;
     return ASG_OK;

@@ -71,3 +71,32 @@ def test_admission_rejects_over_budget_and_cancel():
     rid2 = srv.submit(small, 200)
     assert srv.wait(rid2, 30000.0).status == 0
     srv.close()
+
+
+def test_queued_staged_and_running_cancels_with_admission_thread():
+    """Admission runs on its own thread: requests are prepared while the
+    batch steps, wait for budget in arrival order, and can be cancelled in
+    every state (queued, being admitted, staged, running).  Every request
+    that finishes is bitwise its run alone."""
+    quick = Model(config_path("quick"), pre_time=0.0)
+    uc = Model(config_path("use_case"), seed=7, pre_time=0.0)
+    srv = Server(chunk_steps=64, max_instances=3)  # the rest wait in the queue
+    ids, want = [], []
+    for k in range(12):
+        m = quick if k % 2 else uc
+        steps = 3000 + 500 * k
+        ids.append(srv.submit(m, steps))
+        want.append((m, steps))
+    for k in (1, 6, 11):  # one early (likely running), two later (queued or staged)
+        srv.cancel(ids[k])
+    for k, rid in enumerate(ids):
+        r = srv.wait(rid, 120000.0)
+        if k in (1, 6, 11):
+            assert r.status in (0, 9)  # it may have finished before the cancel landed
+            continue
+        assert r.status == 0, k
+        st, src = srv.fetch_spikes(rid)
+        a_st, a_src = alone(*want[k])
+        assert np.array_equal(st, a_st) and np.array_equal(src, a_src), k
+    assert srv.stats()["resident"] == 0
+    srv.close()
