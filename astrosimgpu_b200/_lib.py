@@ -107,7 +107,8 @@ class State(C.Structure):
 class EngineOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("chunk_steps", C.c_int32), ("block", C.c_int32),
                 ("use_graphs", C.c_int32), ("sic_mode", C.c_int32), ("pdl", C.c_int32),
-                ("push_mode", C.c_int32), ("mem_budget", C.c_uint64), ("occupancy", C.c_int32)]
+                ("push_mode", C.c_int32), ("mem_budget", C.c_uint64), ("occupancy", C.c_int32),
+                ("astro_precision", C.c_int32)]
 
 
 class ServeOpts(C.Structure):
@@ -183,6 +184,9 @@ SIGNATURES = {
                                           C.c_double, C.c_double, C.c_int64, C.c_int64,
                                           C.c_int32, C.c_double, C.c_double, C.c_double,
                                           C.c_double]),
+    "asg_astro_run_bernoulli_f32": (C.c_int, [vp, c_double_p, C.c_double, C.c_int32, C.c_uint64,
+                                              C.c_double, C.c_double, C.c_int64, C.c_int64,
+                                              C.c_double, C.c_double, C.c_double, C.c_double]),
     "asg_astro_pull_state": (C.c_int, [vp, c_double_p, c_double_p, c_double_p]),
     "asg_astro_last_timing": (C.c_int, [vp, c_double_p, c_int64_p]),
     "asg_astro_autotune": (C.c_int, [vp, c_double_p, C.c_double, C.c_int32, C.c_int32,

@@ -126,6 +126,14 @@ class AstroBackend:
         _lib.call("asg_astro_last_timing", self._h, C.byref(ms), C.byref(k))
         return ms.value, k.value
 
+    def run_bernoulli_f32(self, w: ScalingWorkload, first: int, count: int):
+        """The same workload in FP32 (the precision study); returns the
+        steps' device ms and kernels."""
+        _lib.call("asg_astro_run_bernoulli_f32", self._h, _lib.dptr(w.consts), w.h_step,
+                  w.substeps, w.seed, w.p, w.weight, int(first), int(count), w.Ca_tot, w.IP3_0,
+                  w.tau_IP3, w.delta_IP3)
+        return self.last_timing()
+
     def set_shape(self, shape: int):
         """Use launch shape `shape` (raises AsgError outside the valid range)."""
         _lib.call("asg_astro_set_shape", self._h, int(shape))

@@ -23,6 +23,7 @@ EngineConfig config_from(const asg_engine_opts* o) {
         c.push_mode = o->push_mode;
         c.mem_budget = o->mem_budget;
         c.occupancy = o->occupancy;
+        c.astro_fp32 = o->astro_precision == 32;
     }
     return c;
 }

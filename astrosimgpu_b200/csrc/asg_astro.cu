@@ -226,6 +226,73 @@ cudaError_t launch_astro(int shape, int sms, StepArgs a, AstroArrays s, cudaStre
     return cudaGetLastError();
 }
 
+// Precision study: the kernel-scaling workload in FP32 (astro_rk4_f32),
+// four adjacent cells per thread with 128-bit float4 accesses; uniform
+// parameters, Bernoulli input from the same counter RNG draws as the FP64
+// kernel (the event test is exact, so both see the same events).
+__global__ void __launch_bounds__(128, 8) astro_step_kernel_f32(StepArgs a, AstroKf kf, float* Ca,
+                                                                float* IP3, float* h) {
+    const std::int64_t step = *a.step_base + a.step_offset;
+    const float ca_tot = static_cast<float>(a.u.Ca_tot), ip3_0 = static_cast<float>(a.u.IP3_0),
+                tau = static_cast<float>(a.u.tau), delta = static_cast<float>(a.u.delta),
+                weight = static_cast<float>(a.weight);
+    const std::int64_t quads = (a.n + 3) / 4;
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t q = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+         q < quads; q += stride) {
+        const std::int64_t i0 = 4 * q;
+        const bool full = i0 + 4 <= a.n;
+        float c[4], i3[4], hv[4];
+        if (full) {
+            const float4 C4 = reinterpret_cast<const float4*>(Ca)[q];
+            const float4 I4 = reinterpret_cast<const float4*>(IP3)[q];
+            const float4 H4 = reinterpret_cast<const float4*>(h)[q];
+            c[0] = C4.x; c[1] = C4.y; c[2] = C4.z; c[3] = C4.w;
+            i3[0] = I4.x; i3[1] = I4.y; i3[2] = I4.z; i3[3] = I4.w;
+            hv[0] = H4.x; hv[1] = H4.y; hv[2] = H4.z; hv[3] = H4.w;
+        } else {
+            for (int j = 0; j < 4; ++j) {
+                const bool in = i0 + j < a.n;
+                c[j] = in ? Ca[i0 + j] : 0.0f;
+                i3[j] = in ? IP3[i0 + j] : 0.0f;
+                hv[j] = in ? h[i0 + j] : 0.0f;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float in =
+                (mix64(a.seed, static_cast<std::uint64_t>(i0 + j), 1000ULL +
+                       static_cast<std::uint64_t>(step)) >> 11) < a.p_threshold ? weight : 0.0f;
+            astro_rk4_f32(kf, ca_tot, ip3_0, tau, delta, in, 0.0f, c[j], i3[j], hv[j]);
+        }
+        if (full) {
+            reinterpret_cast<float4*>(Ca)[q] = make_float4(c[0], c[1], c[2], c[3]);
+            reinterpret_cast<float4*>(IP3)[q] = make_float4(i3[0], i3[1], i3[2], i3[3]);
+            reinterpret_cast<float4*>(h)[q] = make_float4(hv[0], hv[1], hv[2], hv[3]);
+        } else {
+            for (int j = 0; j < 4 && i0 + j < a.n; ++j) {
+                Ca[i0 + j] = c[j];
+                IP3[i0 + j] = i3[j];
+                h[i0 + j] = hv[j];
+            }
+        }
+    }
+}
+
+// float <-> double copies of the study's state.
+__global__ void narrow_kernel(std::int64_t n, const double* __restrict__ src,
+                              float* __restrict__ dst) {
+    for (std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = static_cast<float>(src[i]);
+}
+__global__ void widen_kernel(std::int64_t n, const float* __restrict__ src,
+                             double* __restrict__ dst) {
+    for (std::int64_t i = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = src[i];
+}
+
 // The drop-in update's kernel for its parameter form, input and noise.
 template <bool kUniform>
 cudaError_t launch_update_p(bool pending, bool noisy, int shape, int sms, const StepArgs& a,
@@ -292,6 +359,10 @@ struct AstroEngine {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DevBuf Ca, IP3, h, input, Ca_tot, IP3_0, tau, inv_tau, delta, step_base;
+    // Precision study: the state rounded to float, valid while no FP64 call
+    // has advanced the FP64 state since (f32_valid).
+    DevBuf Ca32, IP332, h32;
+    bool f32_valid = false;
     double last_ms = 0.0;
     std::int64_t last_kernels = 0;
     int shape = 0;  // launch shape (see kShapes), set by asg_astro_autotune
@@ -511,6 +582,7 @@ int asg_astro_pull_state(asg_astro* s, double* Ca, double* IP3, double* h) {
 }
 
 int asg_astro_push_input(asg_astro* s, const double* ip3_input) {
+    asg::NvtxRange nvtx("astrocyte input push (host to device)");
     asg::clear_error();
     if (s == nullptr || ip3_input == nullptr)
         return asg::fail(ASG_ERR_ARG, "asg_astro_push_input: NULL argument");
@@ -530,6 +602,7 @@ int asg_astro_push_input(asg_astro* s, const double* ip3_input) {
 }
 
 int asg_astro_pull_calcium(asg_astro* s, double* Ca) {
+    asg::NvtxRange nvtx("astrocyte calcium pull (device to host)");
     asg::clear_error();
     if (s == nullptr || Ca == nullptr)
         return asg::fail(ASG_ERR_ARG, "asg_astro_pull_calcium: NULL argument");
@@ -550,6 +623,7 @@ int asg_astro_pull_calcium(asg_astro* s, double* Ca) {
 int asg_astro_update(asg_astro* s, const double* consts, double h_step, int32_t substeps,
                      double noise_std, int32_t independent_noise, double shared_noise,
                      uint64_t noise_seed, uint64_t noise_index) {
+    asg::NvtxRange nvtx("update astrocytes");
     asg::clear_error();
     if (s == nullptr || consts == nullptr)
         return asg::fail(ASG_ERR_ARG, "asg_astro_update: NULL argument");
@@ -608,6 +682,7 @@ int asg_astro_update(asg_astro* s, const double* consts, double h_step, int32_t 
         e->upd_calls += e->pieces();
     }
     e->input_pending = false;
+    e->f32_valid = false;
     ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
     return ASG_OK;
 }
@@ -616,6 +691,7 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
                             uint64_t seed, double p, double weight, int64_t first, int64_t count,
                             int32_t uniform, double Ca_tot, double IP3_0, double tau_IP3,
                             double delta_IP3) {
+    asg::NvtxRange nvtx("update astrocytes (kernel-scaling workload)");
     asg::clear_error();
     if (s == nullptr || consts == nullptr)
         return asg::fail(ASG_ERR_ARG, "asg_astro_run_bernoulli: NULL argument");
@@ -630,6 +706,7 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
     if (!uniform && !e->has_params)
         return asg::fail(ASG_ERR_STATE, "asg_astro_run_bernoulli: no per-cell parameters");
     e->upd_armed = false;
+    e->f32_valid = false;
     // Per-cell parameters that are all equal run as the scalars they are.
     if (!uniform && e->params_uniform) {
         uniform = 1;
@@ -730,6 +807,85 @@ int asg_astro_last_timing(asg_astro* s, double* device_ms, int64_t* kernels) {
     }
     if (device_ms) *device_ms = e->last_ms;
     if (kernels) *kernels = e->last_kernels;
+    return ASG_OK;
+}
+
+int asg_astro_run_bernoulli_f32(asg_astro* s, const double* consts, double h_step,
+                                int32_t substeps, uint64_t seed, double p, double weight,
+                                int64_t first, int64_t count, double Ca_tot, double IP3_0,
+                                double tau_IP3, double delta_IP3) {
+    asg::NvtxRange nvtx("update astrocytes in FP32 (precision study)");
+    asg::clear_error();
+    if (s == nullptr || consts == nullptr)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_run_bernoulli_f32: NULL argument");
+    if (count < 0 || first < 0 || substeps < 0)
+        return asg::fail(ASG_ERR_ARG, "asg_astro_run_bernoulli_f32: negative step range");
+    auto* e = reinterpret_cast<AstroEngine*>(s);
+    if (e->n == 0 || count == 0) {
+        e->last_ms = 0.0;
+        e->last_kernels = 0;
+        return ASG_OK;
+    }
+    ASG_CUDA(e->join_copies());
+    e->upd_armed = false;
+    const std::size_t fbytes = static_cast<std::size_t>(e->n) * sizeof(float);
+    const int cgrid = e->sms * 8;
+    if (e->Ca32.get() == nullptr) {
+        ASG_TRY(e->Ca32.alloc(fbytes, false));
+        ASG_TRY(e->IP332.alloc(fbytes, false));
+        ASG_TRY(e->h32.alloc(fbytes, false));
+    }
+    if (!e->f32_valid) {
+        asg::narrow_kernel<<<cgrid, 256, 0, e->stream>>>(e->n, e->Ca.as<double>(), e->Ca32.as<float>());
+        asg::narrow_kernel<<<cgrid, 256, 0, e->stream>>>(e->n, e->IP3.as<double>(), e->IP332.as<float>());
+        asg::narrow_kernel<<<cgrid, 256, 0, e->stream>>>(e->n, e->h.as<double>(), e->h32.as<float>());
+        ASG_CUDA(cudaGetLastError());
+    }
+    asg::StepArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n = e->n;
+    a.k = asg::make_astro_k(consts, h_step, substeps);
+    a.u = asg::UniformParams{Ca_tot, IP3_0, tau_IP3, delta_IP3, 1.0 / tau_IP3};
+    a.seed = seed;
+    a.p = p;
+    a.p_threshold = asg::bernoulli_threshold(p);
+    a.weight = weight;
+    a.step_base = e->step_base.as<std::int64_t>();
+    const asg::AstroKf kf = asg::astro_k_f32(a.k);
+    const std::int64_t quads = (e->n + 3) / 4;
+    const int grid = static_cast<int>(std::max<std::int64_t>(
+        1, std::min<std::int64_t>((quads + 127) / 128, static_cast<std::int64_t>(e->sms) * 8 * 4)));
+    std::int64_t base = first;
+    ASG_CUDA(cudaMemcpyAsync(e->step_base.get(), &base, sizeof base, cudaMemcpyHostToDevice,
+                             e->stream));
+    // Plain launches of 64-step groups, the step read from the device
+    // counter; the counter advances by a one-thread kernel after each group.
+    ASG_CUDA(cudaEventRecord(e->ev0, e->stream));
+    std::int64_t done = 0, kernels = 0;
+    while (done < count) {
+        const int chunk = static_cast<int>(std::min<std::int64_t>(64, count - done));
+        for (int j = 0; j < chunk; ++j) {
+            a.step_offset = j;
+            asg::astro_step_kernel_f32<<<grid, 128, 0, e->stream>>>(
+                a, kf, e->Ca32.as<float>(), e->IP332.as<float>(), e->h32.as<float>());
+        }
+        asg::advance_counter_kernel<<<1, 1, 0, e->stream>>>(e->step_base.as<std::int64_t>(), chunk);
+        ASG_CUDA(cudaGetLastError());
+        done += chunk;
+        kernels += chunk + 1;
+    }
+    ASG_CUDA(cudaEventRecord(e->ev1, e->stream));
+    // The FP64 state holds the widened result, for pulls and FP64 calls.
+    asg::widen_kernel<<<cgrid, 256, 0, e->stream>>>(e->n, e->Ca32.as<float>(), e->Ca.as<double>());
+    asg::widen_kernel<<<cgrid, 256, 0, e->stream>>>(e->n, e->IP332.as<float>(), e->IP3.as<double>());
+    asg::widen_kernel<<<cgrid, 256, 0, e->stream>>>(e->n, e->h32.as<float>(), e->h.as<double>());
+    ASG_CUDA(cudaGetLastError());
+    ASG_CUDA(cudaStreamSynchronize(e->stream));
+    e->f32_valid = true;
+    float ms = 0.0f;
+    ASG_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    e->last_ms = ms;
+    e->last_kernels = kernels;
     return ASG_OK;
 }
 

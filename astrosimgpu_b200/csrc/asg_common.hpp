@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdarg>
 #include <cstdint>
@@ -38,6 +39,19 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 // the (n+1)-th device allocation of the process fails with out-of-memory.
 // Lets the host error paths be exercised without exhausting a shared GPU.
 bool injected_alloc_failure();
+
+// Host-side NVTX range over a scope, named after the reference's phase
+// table where one applies (Network::run's PhaseProfile, network.hpp:32-45:
+// "update astrocytes", "SIC gather+deliver", ...).  Seen by Nsight Systems
+// and by ncu's --nvtx filters; costs a call into the NVTX stub when no tool
+// is attached.
+class NvtxRange {
+public:
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Owning device allocation (cudaMalloc / cudaFree), zero-filled on request.
 class DevBuf {

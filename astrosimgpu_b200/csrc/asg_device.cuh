@@ -279,6 +279,98 @@ __device__ __forceinline__ void astro_rk4(const AstroK& k, double ca_tot, double
     }
 }
 
+// ------------------------------------- Li-Rinzel in FP32 (precision study)
+//
+// The reference's precision question (docs/experiments.md, "Single or double
+// precision"): is FP32 enough for the Li-Rinzel calcium dynamics, whose ER
+// calcium (Ca_tot - Ca) / ratio_ER_cyt subtracts quantities of similar size?
+// Its method is `real = float` throughout.  This is that form for the
+// astrocyte: state rounded to float, every operation of the right-hand side
+// and of the RK4 stages in float, IEEE float division, the same operation
+// order.  It is an opt-in study form, never the default and never compared
+// bitwise: the FP64 path above is the product.
+struct AstroKf {
+    float Kd_IP3_1, Kd_IP3_2, Kd_act, ratio_ER_cyt, chan, serca, km2, leak, ah, k_IP3R;
+    float half_h, h, h6;
+    int substeps;
+};
+
+__host__ __device__ inline AstroKf astro_k_f32(const AstroK& k) {
+    AstroKf f;
+    f.Kd_IP3_1 = static_cast<float>(k.Kd_IP3_1);
+    f.Kd_IP3_2 = static_cast<float>(k.Kd_IP3_2);
+    f.Kd_act = static_cast<float>(k.Kd_act);
+    f.ratio_ER_cyt = static_cast<float>(k.ratio_ER_cyt);
+    f.chan = static_cast<float>(k.chan);
+    f.serca = static_cast<float>(k.serca);
+    f.km2 = static_cast<float>(k.km2);
+    f.leak = static_cast<float>(k.leak);
+    f.ah = static_cast<float>(k.ah);
+    f.k_IP3R = static_cast<float>(k.k_IP3R);
+    f.half_h = static_cast<float>(k.half_h);
+    f.h = static_cast<float>(k.h);
+    f.h6 = static_cast<float>(k.h6);
+    f.substeps = k.substeps;
+    return f;
+}
+
+__device__ __forceinline__ void astro_rk4_f32(const AstroKf& k, float ca_tot, float ip3_0,
+                                              float tau, float delta, float input, float noise,
+                                              float& ca, float& ip3, float& hh) {
+    auto rhs = [&](float c, float i3, float hv, float& dCa, float& dIP3, float& dh) {
+        const float er = (ca_tot - c) / k.ratio_ER_cyt;
+        const float ip3_k1 = i3 + k.Kd_IP3_1;
+        const float m = i3 / ip3_k1;
+        const float n = c / (c + k.Kd_act);
+        const float m3 = m * m * m;
+        const float n3 = n * n * n;
+        const float h3 = hv * hv * hv;
+        const float gradient = er - c;
+        const float release = k.chan * m3 * n3 * h3 * gradient;
+        const float ca2 = c * c;
+        const float uptake = k.serca * c * c / (k.km2 + ca2);
+        const float leak = k.leak * gradient;
+        const float open_rate = k.ah * ip3_k1 / (i3 + k.Kd_IP3_2);
+        const float close_rate = k.k_IP3R * c;
+        dCa = release - uptake + leak + noise;
+        dIP3 = (ip3_0 - i3) / tau;
+        dh = open_rate * (1.0f - hv) - close_rate * hv;
+    };
+    if (input != 0.0f) ip3 += delta * input;
+    for (int s = 0; s < k.substeps; ++s) {
+        float sCa = 0.0f, sIP3 = 0.0f, sh = 0.0f;
+        float xCa = ca, xIP3 = ip3, xh = hh;
+#pragma unroll
+        for (int st = 0; st < 4; ++st) {
+            float rCa, rIP3, rh;
+            rhs(xCa, xIP3, xh, rCa, rIP3, rh);
+            if (st == 0) {
+                sCa = rCa;
+                sIP3 = rIP3;
+                sh = rh;
+            } else if (st < 3) {
+                sCa = sCa + 2.0f * rCa;
+                sIP3 = sIP3 + 2.0f * rIP3;
+                sh = sh + 2.0f * rh;
+            } else {
+                sCa = sCa + rCa;
+                sIP3 = sIP3 + rIP3;
+                sh = sh + rh;
+            }
+            const float step = st < 2 ? k.half_h : k.h;
+            xCa = ca + step * rCa;
+            xIP3 = ip3 + step * rIP3;
+            xh = hh + step * rh;
+        }
+        ca += k.h6 * sCa;
+        ip3 += k.h6 * sIP3;
+        hh += k.h6 * sh;
+        ca = ca < 0.0f ? 0.0f : (ca > ca_tot ? ca_tot : ca);
+        hh = hh < 0.0f ? 0.0f : (hh > 1.0f ? 1.0f : hh);
+        ip3 = ip3 < 0.0f ? 0.0f : ip3;
+    }
+}
+
 // ---------------------------------------------------------------- AdEx
 
 // Population constants of one neuron population.

@@ -149,6 +149,7 @@ __global__ void ring_pack_kernel(const std::uint32_t* __restrict__ st,
 // with r.words known (the stream synchronised once for it).
 int build_in_ring(std::uint32_t n_src, const std::uint32_t* rs, const std::uint32_t* tg,
                   std::uint32_t n_targets, cudaStream_t st, InRingDev& r) {
+    NvtxRange nvtx("admission: in-edge numbering (arrival rings)");
     const std::uint32_t m = rs[n_src];
     const std::uint32_t n = n_targets;
     r.m = m;
@@ -493,6 +494,7 @@ int Engine::commit(std::unique_ptr<Instance> inst, int* id_out) {
 int Engine::prepare(const asg_network_desc& d, const asg_record_opts* rec, std::int64_t first,
                     std::int64_t end, bool keep_spikes, bool check_budget,
                     std::unique_ptr<Instance>* out) {
+    NvtxRange nvtx("admission: prepare instance");
     // Touches no state the chunks in flight use: the tables are prepared and
     // uploaded on the upload stream into a new arena, so a serving loop can
     // run this on another thread while the engine's stream keeps stepping.
@@ -650,6 +652,7 @@ int Engine::prepare(const asg_network_desc& d, const asg_record_opts* rec, std::
         }
     }
     D.astro_uniform = uniform ? 1 : 0;
+    D.astro_fp32 = cfg.astro_fp32 ? 1 : 0;
     D.Ca_tot_u = uval[0];
     D.IP3_0_u = uval[1];
     D.tau_u = uval[2];
@@ -1030,6 +1033,8 @@ int Engine::capture_graph(int steps) {
 // stream at the end, so nothing of a chunk outlives it.  The first step of a
 // chunk follows the descriptor copy: no early (programmatic) launch for it.
 cudaError_t Engine::issue_steps(int steps) {
+    NvtxRange nvtx("step chain: arrival application, background input, update astrocytes, "
+                   "update neurons, spike delivery, SIC gather+deliver");
     const bool side_on = !side_work.empty();
     const int G = kSicBatchSteps;
     cudaError_t e = cudaSuccess;
@@ -1138,6 +1143,7 @@ int Engine::launch_chunk(int parity, int steps) {
 }
 
 int Engine::collect(int parity) {
+    NvtxRange nvtx("collect: spikes and recorded rows to the recorder");
     if (!pending[parity]) return ASG_OK;
     ASG_CUDA(cudaEventSynchronize(ev_chunk[parity]));
     pending[parity] = false;
@@ -1227,6 +1233,7 @@ int Engine::run_chunk(std::int64_t max_steps) {
 }
 
 int Engine::run(std::int64_t n_steps) {
+    NvtxRange nvtx("Network::run (engine)");
     if (n_steps < 0) return fail(ASG_ERR_ARG, "negative step count");
     if (dirty) ASG_TRY(rebuild());
     last_kernels = 0;

@@ -112,6 +112,7 @@ struct InstDev {
     // astrocytes
     AstroK ak;
     std::int32_t astro_uniform;
+    std::int32_t astro_fp32;  // precision study: the astrocyte update in FP32
     double Ca_tot_u, IP3_0_u, tau_u, delta_u, inv_tau_u;
     double a_rate, a_weight, a_lambda, a_limit, a_std;
     std::int32_t a_indep, a_steps_per_noise;

@@ -62,6 +62,7 @@ struct EngineConfig {
     std::uint64_t mem_budget = 0;
     int occupancy = 0;  // 0 auto, 1 latency form, 2 high-occupancy form of the step kernel
     bool large_total = false;  // the engine will hold 2^16+ neurons in all (auto SIC form)
+    bool astro_fp32 = false;   // precision study: astrocyte update in FP32
 };
 
 class Engine {

@@ -831,6 +831,22 @@ __device__ __noinline__ void help_push(const InstDev& I, const StepInfo& S, cons
                 static_cast<std::uint32_t>(I.push_blocks + I.push_helpers));
 }
 
+// The precision study's astrocyte update (astro_rk4_f32): state, parameters
+// and input rounded to float, the update in float, the result held as the
+// double of that float.  Out of line: the FP64 path carries none of it.
+__device__ __noinline__ void astro_update_f32(const InstDev& I, double ca_tot, double ip3_0,
+                                              double tau, double delta, double input,
+                                              double noise, double& ca, double& ip3,
+                                              double& hh) {
+    float c = static_cast<float>(ca), i3 = static_cast<float>(ip3), hv = static_cast<float>(hh);
+    astro_rk4_f32(astro_k_f32(I.ak), static_cast<float>(ca_tot), static_cast<float>(ip3_0),
+                  static_cast<float>(tau), static_cast<float>(delta), static_cast<float>(input),
+                  static_cast<float>(noise), c, i3, hv);
+    ca = c;
+    ip3 = i3;
+    hh = hv;
+}
+
 template <bool kPdl>
 __device__ void astro_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     const std::uint32_t a = wk.first + threadIdx.x;
@@ -873,7 +889,10 @@ __device__ void astro_role(const InstDev& I, const StepInfo& S, const Work& wk) 
     }
     if (ev > 0) ip3_in += I.a_weight * static_cast<double>(ev);
     // AstrocytePopulation::update (astrocyte.cpp:307-329)
-    astro_rk4<false>(I.ak, ca_tot, ip3_0, tau, inv_tau, delta, ip3_in, noise, ca, ip3, hh);
+    if (I.astro_fp32)
+        astro_update_f32(I, ca_tot, ip3_0, tau, delta, ip3_in, noise, ca, ip3, hh);
+    else
+        astro_rk4<false>(I.ak, ca_tot, ip3_0, tau, inv_tau, delta, ip3_in, noise, ca, ip3, hh);
     I.Ca[a] = ca;
     I.IP3[a] = ip3;
     I.h[a] = hh;

@@ -36,6 +36,7 @@ void usage(const char* argv0) {
               << "  -p, --pre-time MS     discarded transient     [from config]\n"
               << "  -a, --astrocytes N    override the astrocyte count [from config]\n"
               << "      --chunk N         steps per captured CUDA graph [by network size]\n"
+              << "      --astro-fp32      astrocyte update in FP32 (precision study) [FP64]\n"
               << "      --no-analysis     skip the post-run summary\n"
               << "  -h, --help            show this message\n";
 }
@@ -56,6 +57,7 @@ int main(int argc, char** argv) {
     double sim = -1.0, pre = -1.0;
     bool analysis = true;
     int chunk = 0;  // 0: the engine's default for the network size
+    bool astro_fp32 = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         auto next = [&]() -> std::string {
@@ -82,6 +84,8 @@ int main(int argc, char** argv) {
             astro = std::stoll(next());
         } else if (a == "--chunk") {
             chunk = std::stoi(next());
+        } else if (a == "--astro-fp32") {
+            astro_fp32 = true;
         } else if (a == "--no-analysis") {
             analysis = false;
         } else {
@@ -144,6 +148,7 @@ int main(int argc, char** argv) {
     asg_engine_opts opts;
     std::memset(&opts, 0, sizeof opts);
     opts.chunk_steps = chunk;
+    opts.astro_precision = astro_fp32 ? 32 : 64;
     asg_network* net = nullptr;
     if (!ok(asg_create(&desc, &rec, &opts, &net), "create")) return 1;
     std::cout << "Simulating " << sc[6] << " ms transient + " << sc[7] << " ms recorded ...\n";
@@ -271,7 +276,9 @@ int main(int argc, char** argv) {
     os << "neuron -> astrocyte    " << st5[2] << "\n";
     os << "astrocyte -> neuron    " << st5[3] << "\n\n";
     os << "dt                    " << dt << " ms (" << desc.substeps << " substeps)\n";
-    os << "astrocyte backend     B200 native (sm_100a, FP64), whole step on the GPU\n";
+    os << "astrocyte backend     B200 native (sm_100a, "
+       << (astro_fp32 ? "FP64 neurons, FP32 astrocytes: precision study" : "FP64")
+       << "), whole step on the GPU\n";
     os << "transient             " << sc[6] << " ms\n";
     os << "recorded              " << sc[7] << " ms\n";
     os << "seed                  " << static_cast<unsigned long long>(sc[2]) << "\n\n";

@@ -60,12 +60,12 @@ BYTES_PER_CELL_STEP = 48  # Ca, IP3, h: read + write, FP64
 # an ncu capture of the headline workload (profiles/astro_step_kernel_N1e7.md):
 # FP64 thread instructions executed (DADD + DMUL + DFMA + the rest of the
 # FP64 pipe) and FP64 flops (DFMA counted twice).
-FP64_INST_PER_CELL_STEP = None
-FP64_FLOP_PER_CELL_STEP = None
+FP64_INST_PER_CELL_STEP = 313  # 64 DADD + 109 DMUL + 134 DFMA + 6 other
+FP64_FLOP_PER_CELL_STEP = 441
 FP64_LANES_PER_SM = 64
 # dram__bytes_read.sum + dram__bytes_write.sum of one astro_step_kernel launch
 # at N = 1e7, from the same capture.
-NCU_TRAFFIC_PER_LAUNCH = {10_000_000: 420_363_392}
+NCU_TRAFFIC_PER_LAUNCH = {10_000_000: 420_352_512}
 
 
 def load_peaks():

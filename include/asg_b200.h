@@ -171,6 +171,10 @@ typedef struct asg_engine_opts {
                                trips, 128 registers), 2 high-occupancy form
                                (6 blocks of 128 threads per SM; block 128 only).
                                Both forms give the same bits.                  */
+    int32_t astro_precision;/* 0 or 64: FP64 (the product); 32: the astrocyte
+                               update in FP32 -- the reference's precision
+                               study (docs/experiments.md), opt-in, not
+                               bitwise to anything                             */
 } asg_engine_opts;
 
 /* ------------------------------------------------------ single network
@@ -303,6 +307,18 @@ int asg_astro_run_bernoulli(asg_astro* s, const double* consts, double h_step, i
                             uint64_t seed, double p, double weight, int64_t first, int64_t count,
                             int32_t uniform, double Ca_tot, double IP3_0, double tau_IP3,
                             double delta_IP3);
+/* Precision study (the reference's docs/experiments.md, "Single or double
+ * precision": is FP32 enough for the Li-Rinzel dynamics?).  The same
+ * workload with uniform parameters, the state rounded to float on entry (or
+ * kept in float from the previous call of this entry point) and advanced in
+ * FP32 arithmetic; the handle's FP64 state receives the widened result.
+ * Device time of the steps alone in asg_astro_last_timing.  No counterpart
+ * in the reference's GPU backend (the reference runs the study by rebuilding
+ * with `real = float`); not bitwise to anything. */
+int asg_astro_run_bernoulli_f32(asg_astro* s, const double* consts, double h_step,
+                                int32_t substeps, uint64_t seed, double p, double weight,
+                                int64_t first, int64_t count, double Ca_tot, double IP3_0,
+                                double tau_IP3, double delta_IP3);
 /* Read the state without destroying the handle. */
 int asg_astro_pull_state(asg_astro* s, double* Ca, double* IP3, double* h);
 /* Time the kernel's launch shapes (cells per thread, block size, register
