@@ -640,6 +640,8 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
         I.dgin[c] = dgin;
         I.refr[c] = refr;
 
+        double v0 = 0.0, v1 = 0.0;  // the values a spike's edges deliver
+        std::uint32_t r1 = 0;
         if (spiked) {
             // Tsodyks-Markram update of this source (network.cpp:230-247); the
             // value its edges deliver is w*x*u per set.
@@ -656,36 +658,75 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
                 I.stp_u[c] = u;
                 I.stp_t[c] = t_now;
             }
-            const double v0 =
-                exc ? (I.stp_on ? I.w_e * x * u : I.w_e) : (I.stp_on ? I.w_i * x * u : I.w_i);
-            const double v1 = exc ? (I.stp_on ? I.w_n2a * x * u : I.w_n2a) : 0.0;
-            if (I.deferred_push) {
-                // n2a row start of an excitatory source (~0: inhibitory),
-                // loaded while the append's atomic is in flight
-                const std::uint32_t r1 = exc ? __ldg(I.n2a_rs + c) : kNoBit;
-                const unsigned long long old = atomicAdd(
-                    I.spk_packed + S.ls * kHeaderStride,
-                    (1ull << 40) | static_cast<unsigned long long>(len0 + len1));
-                const std::size_t o = static_cast<std::size_t>(S.ls) * I.N + (old >> 40);
-                *reinterpret_cast<uint4*>(I.spk_meta + 4 * o) =
-                    make_uint4(r1, static_cast<std::uint32_t>(old & 0xFFFFFFFFFFull), r0, len0);
-                *reinterpret_cast<double2*>(I.spk_val + 2 * o) = make_double2(v0, v1);
-            } else {
+            v0 = exc ? (I.stp_on ? I.w_e * x * u : I.w_e) : (I.stp_on ? I.w_i * x * u : I.w_i);
+            v1 = exc ? (I.stp_on ? I.w_n2a * x * u : I.w_n2a) : 0.0;
+            // n2a row start of an excitatory source (~0: inhibitory), loaded
+            // while the warp's append is formed
+            if (I.deferred_push) r1 = exc ? __ldg(I.n2a_rs + c) : kNoBit;
+            if (!I.deferred_push) {
                 s_val[threadIdx.x * 2 + 0] = v0;
                 s_val[threadIdx.x * 2 + 1] = v1;
                 const int pos = atomicAdd(&s_nspk, 1);
                 s_spk[pos] = threadIdx.x;
             }
-            if (I.rec_spikes && step >= I.rec_from) {
-                const unsigned long long li = atomicAdd(I.spike_log_n, 1ULL);
-                if (li < I.spike_log_cap) {
-                    I.spike_log[li] = (static_cast<unsigned long long>(step) << 32) | c;
-                } else {
-                    atomicAdd(I.counters + 3, 1ULL);
+        }
+
+        // The warp's spikes are compacted with a ballot and prefix sums: one
+        // atomic per warp reserves the spike records and edge range of the
+        // deferred push, one the spike-log entries, one each counter; every
+        // spiking lane writes at its rank among the warp's spiking lanes
+        // (ascending source) and at its exclusive prefix of edge counts.
+        // The active lanes of a warp are a prefix of it (threadIdx.x <
+        // wk.count), all of which reach this point.
+        const unsigned lane = threadIdx.x & 31u;
+        const unsigned wbase = threadIdx.x & ~31u;
+        const unsigned left = wk.count - wbase;  // > 0 for an active lane
+        const unsigned act = left >= 32u ? 0xFFFFFFFFu : ((1u << left) - 1u);
+        __syncwarp(act);
+        const unsigned smask = __ballot_sync(act, spiked);
+        if (smask != 0u) {
+            const unsigned rank = __popc(smask & ((1u << lane) - 1u));
+            const int leader = __ffs(smask) - 1;
+            const unsigned nspk = __popc(smask);
+            const unsigned long long edges =
+                spiked ? static_cast<unsigned long long>(len0 + len1) : 0ull;
+            unsigned long long incl = edges;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const unsigned long long t = __shfl_up_sync(act, incl, d);
+                if (lane >= static_cast<unsigned>(d)) incl += t;
+            }
+            const int last = 31 - __clz(act);
+            const unsigned long long total = __shfl_sync(act, incl, last);
+            unsigned long long base_spk = 0, base_log = 0;
+            const bool logging = I.rec_spikes && step >= I.rec_from;
+            if (lane == static_cast<unsigned>(leader)) {
+                if (I.deferred_push)
+                    base_spk = atomicAdd(I.spk_packed + S.ls * kHeaderStride,
+                                         (static_cast<unsigned long long>(nspk) << 40) | total);
+                if (logging) base_log = atomicAdd(I.spike_log_n, static_cast<unsigned long long>(nspk));
+                atomicAdd(I.counters + 0, total);
+                atomicAdd(I.counters + 2, static_cast<unsigned long long>(nspk));
+            }
+            base_spk = __shfl_sync(act, base_spk, leader);
+            base_log = __shfl_sync(act, base_log, leader);
+            if (spiked) {
+                if (I.deferred_push) {
+                    const std::size_t o = static_cast<std::size_t>(S.ls) * I.N + (base_spk >> 40) + rank;
+                    const unsigned long long eoff = (base_spk & 0xFFFFFFFFFFull) + (incl - edges);
+                    *reinterpret_cast<uint4*>(I.spk_meta + 4 * o) =
+                        make_uint4(r1, static_cast<std::uint32_t>(eoff), r0, len0);
+                    *reinterpret_cast<double2*>(I.spk_val + 2 * o) = make_double2(v0, v1);
+                }
+                if (logging) {
+                    const unsigned long long li = base_log + rank;
+                    if (li < I.spike_log_cap) {
+                        I.spike_log[li] = (static_cast<unsigned long long>(step) << 32) | c;
+                    } else {
+                        atomicAdd(I.counters + 3, 1ULL);
+                    }
                 }
             }
-            atomicAdd(I.counters + 0, static_cast<unsigned long long>(len0 + len1));
-            atomicAdd(I.counters + 2, 1ULL);
         }
 
         if (I.rec_neuron_max > 0 && c < I.rec_neuron_max && S.rec_now) {
