@@ -971,6 +971,14 @@ int Engine::rebuild() {
     wide = cfg.block == 128 &&
            (cfg.occupancy == 2 ||
             (cfg.occupancy == 0 && work.size() > static_cast<std::size_t>(2 * 4 * sms)));
+    // The high-occupancy form runs as one wave of resident blocks, each
+    // taking several work items (no per-item block launch or descriptor
+    // staging after its first).
+    wide_grid = 0;
+    if (wide && cfg.item_loop) {
+        const int nb = step_wide_blocks_per_sm();
+        if (nb > 0) wide_grid = nb * sms;
+    }
     persistent_grid = 0;
     if (cfg.use_graphs == 2 && !work.empty()) {
         const int cap = persistent_blocks(B);
@@ -1060,7 +1068,7 @@ cudaError_t Engine::issue_steps(int steps) {
             e = cudaStreamWaitEvent(stream, ev_side_done[((k - side_lead) / G) % kSideEvents], 0);
         if (e == cudaSuccess)
             e = launch_step(d_insts.as<InstDev>(), d_work.as<Work>(), static_cast<int>(work.size()),
-                            cfg.block, k, cfg.pdl && k > 0, wide, stream);
+                            cfg.block, k, cfg.pdl && k > 0, wide, wide_grid, stream);
     }
     if (side_on && e == cudaSuccess) {
         e = cudaEventRecord(ev_side_join, side);

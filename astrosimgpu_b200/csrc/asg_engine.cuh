@@ -205,7 +205,11 @@ cudaError_t launch_sic_batch(const InstDev* insts, const Work* work, int n_work,
 // of the stream is still running (the kernel waits for it before any access
 // to instance state).
 // `wide`: the high-occupancy form (block 128 only; same arithmetic).
+// One step launch over the work table.  max_grid > 0 caps the grid (blocks
+// then run several work items each); 0 launches one block per item.
 cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
-                        bool pdl, bool wide, cudaStream_t stream);
+                        bool pdl, bool wide, int max_grid, cudaStream_t stream);
+// Resident blocks per SM of the high-occupancy step kernel form (128 threads).
+int step_wide_blocks_per_sm();
 
 }  // namespace asg

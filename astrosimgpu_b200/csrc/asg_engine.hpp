@@ -63,6 +63,7 @@ struct EngineConfig {
     int occupancy = 0;  // 0 auto, 1 latency form, 2 high-occupancy form of the step kernel
     bool large_total = false;  // the engine will hold 2^16+ neurons in all (auto SIC form)
     bool astro_fp32 = false;   // precision study: astrocyte update in FP32
+    bool item_loop = true;     // high-occupancy form: one wave, several items per block
 };
 
 class Engine {
@@ -149,6 +150,7 @@ private:
     std::vector<std::pair<int, cudaGraphExec_t>> graphs;
     bool graph_mode() const { return cfg.use_graphs == 0 || cfg.use_graphs == 1; }
     bool wide = false;  // launches use the high-occupancy form of the step kernel
+    int wide_grid = 0;  // its grid: one wave of resident blocks (0: one block per item)
     cudaGraphExec_t find_graph(int steps);
     int capture_graph(int steps);
     void drop_graphs();

@@ -1009,31 +1009,46 @@ __device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, co
 }
 
 // One step of every resident instance (the body of both kernel forms below).
+// Block b runs work items b, b + gridDim.x, ...: one item per block when the
+// grid covers the work table (a step of a few waves), several when the grid
+// is one wave of resident blocks (a large step), which saves the per-block
+// staging and scheduling of the items after the first.  No item waits on
+// another within a launch, so any assignment of items to blocks is valid.
 __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
-                                          const Work* __restrict__ work, int k) {
-    // Stage this block's instance descriptor and step arithmetic in shared
-    // memory.  Both depend only on data written before the chunk started, so
-    // this overlaps the tail of the previous step's grid.
+                                          const Work* __restrict__ work, int k, int n_work) {
+    // Stage the item's instance descriptor and step arithmetic in shared
+    // memory (again only when the instance changes).  Both depend only on
+    // data written before the chunk started, so this overlaps the tail of
+    // the previous step's grid.
     __shared__ __align__(16) unsigned char s_raw[sizeof(InstDev)];
     __shared__ StepInfo s_info;
-    // Through L2 (never a cached line of an earlier chunk or engine): the
-    // descriptors are rewritten by a host copy before every chunk.
-    const Work wk = load_work(work + blockIdx.x);
-    {
-        const auto* src = reinterpret_cast<const std::uint32_t*>(insts + wk.inst);
-        auto* dst = reinterpret_cast<std::uint32_t*>(s_raw);
-        for (unsigned i = threadIdx.x; i < sizeof(InstDev) / 4; i += blockDim.x)
-            dst[i] = __ldcg(src + i);
-    }
-    __syncthreads();
     const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
-    if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
-    __syncthreads();
-    // Programmatic dependent launch: let the next step's grid be scheduled
-    // now.  Each role waits (griddepcontrol.wait) for this launch's
-    // predecessor to complete before touching state it writes.
-    asm volatile("griddepcontrol.launch_dependents;");
-    run_role<true>(I, s_info, wk);
+    std::uint32_t staged = 0xFFFFFFFFu;
+    for (int wi = blockIdx.x; wi < n_work; wi += gridDim.x) {
+        // Through L2 (never a cached line of an earlier chunk or engine):
+        // the descriptors are rewritten by a host copy before every chunk.
+        const Work wk = load_work(work + wi);
+        if (wk.inst != staged) {  // block-uniform
+            __syncthreads();      // the previous item is done with s_raw / s_info
+            const auto* src = reinterpret_cast<const std::uint32_t*>(insts + wk.inst);
+            auto* dst = reinterpret_cast<std::uint32_t*>(s_raw);
+            for (unsigned i = threadIdx.x; i < sizeof(InstDev) / 4; i += blockDim.x)
+                dst[i] = __ldcg(src + i);
+            __syncthreads();
+            if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
+            __syncthreads();
+            if (staged == 0xFFFFFFFFu) {
+                // Programmatic dependent launch: let the next step's grid be
+                // scheduled now.  Each role waits (griddepcontrol.wait) for
+                // this launch's predecessor to complete before touching
+                // state it writes.
+                asm volatile("griddepcontrol.launch_dependents;");
+            }
+            staged = wk.inst;
+        }
+        run_role<true>(I, s_info, wk);
+        __syncthreads();  // the role's shared arrays are free for the next item
+    }
 }
 
 // Two forms of the step kernel, same arithmetic: step_kernel allows blocks of
@@ -1043,14 +1058,15 @@ __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
 // registers, some spilled: more warps to hide latency when a step is many
 // waves of blocks).
 __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restrict__ insts,
-                                                         const Work* __restrict__ work, int k) {
-    step_body(insts, work, k);
+                                                         const Work* __restrict__ work, int k,
+                                                         int n_work) {
+    step_body(insts, work, k, n_work);
 }
 
 __global__ void __launch_bounds__(128, 6) step_kernel_wide(const InstDev* __restrict__ insts,
-                                                           const Work* __restrict__ work,
-                                                           int k) {
-    step_body(insts, work, k);
+                                                           const Work* __restrict__ work, int k,
+                                                           int n_work) {
+    step_body(insts, work, k, n_work);
 }
 
 // Grid-wide barrier of the persistent chunk kernel (all blocks co-resident
@@ -1254,10 +1270,17 @@ cudaError_t launch_chunk_persistent(const InstDev* insts, const Work* work, int 
     return cudaLaunchKernelEx(&cfg, chunk_kernel, insts, work, n_work, steps, gb);
 }
 
+int step_wide_blocks_per_sm() {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step_kernel_wide, 128, 0) != cudaSuccess)
+        return 0;
+    return nb;
+}
+
 cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
-                        bool pdl, bool wide, cudaStream_t stream) {
+                        bool pdl, bool wide, int max_grid, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(static_cast<unsigned>(n_work));
+    cfg.gridDim = dim3(static_cast<unsigned>(max_grid > 0 ? std::min(n_work, max_grid) : n_work));
     cfg.blockDim = dim3(static_cast<unsigned>(block));
     cfg.dynamicSmemBytes = 0;
     cfg.stream = stream;
@@ -1266,8 +1289,9 @@ cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int 
     attr[0].val.programmaticStreamSerializationAllowed = pdl ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (wide && block == 128) return cudaLaunchKernelEx(&cfg, step_kernel_wide, insts, work, k);
-    return cudaLaunchKernelEx(&cfg, step_kernel, insts, work, k);
+    if (wide && block == 128)
+        return cudaLaunchKernelEx(&cfg, step_kernel_wide, insts, work, k, n_work);
+    return cudaLaunchKernelEx(&cfg, step_kernel, insts, work, k, n_work);
 }
 
 }  // namespace asg
