@@ -1071,10 +1071,20 @@ __global__ void __launch_bounds__(128, 6) step_kernel_wide(const InstDev* __rest
 
 // Grid-wide barrier of the persistent chunk kernel (all blocks co-resident
 // by cooperative launch).  Sense by generation count; every wait is bounded:
-// a block that polls kBarrierPolls times without release sets the error word
+// a block still waiting after kBarrierWaitNs (or kBarrierPolls polls) sets the error word
 // and the whole grid stops at its next barrier, so a fault can only end the
 // launch early, never hang it.
-constexpr unsigned kBarrierPolls = 1u << 24;  // x ~64 ns sleep: ~1 s
+// The wait is bounded by time: 1 s on the GPU's global timer (ns).  A poll
+// count bounds it as well, as a backstop that does not depend on the timer
+// (each poll sleeps ~64 ns and makes an acquire load: well above 1 s).
+constexpr unsigned long long kBarrierWaitNs = 1000000000ull;
+constexpr unsigned kBarrierPolls = 1u << 26;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
@@ -1095,8 +1105,10 @@ __device__ bool grid_sync(GridBarrier* gb, unsigned nblocks) {
             atomicAdd(&gb->gen, 1u);
         } else {
             unsigned polls = 0;
+            const unsigned long long t0 = global_ns();
             while (ld_acquire(&gb->gen) == gen) {
-                if (++polls > kBarrierPolls || ld_acquire(&gb->error) != 0) {
+                if (++polls > kBarrierPolls || ld_acquire(&gb->error) != 0 ||
+                    global_ns() - t0 > kBarrierWaitNs) {
                     atomicExch(&gb->error, 1u);
                     ok = 0;
                     break;

@@ -22,7 +22,9 @@ def test_grid_barrier_wait_is_bounded_and_reported():
     ms = C.c_double()
     assert lib.asg_selftest_barrier_timeout(C.byref(t), C.byref(ms)) == 0
     assert t.value == 1            # the blocks gave up and said so
-    assert ms.value < 20000.0      # within the bound, no hang
+    # the wait is bounded at 1 s on the GPU's global timer: the launch ends
+    # shortly after it
+    assert 900.0 <= ms.value < 2500.0, ms.value
     # the context is still usable afterwards
     n = Network(Model(config_path("quick"), pre_time=0.0), use_graphs=2)
     n.step(100)
