@@ -766,6 +766,7 @@ int Engine::prepare(const asg_network_desc& d, const asg_record_opts* rec, std::
     add_seg(D.sic_soff, sic.soff.size() * 4, sic.soff.data());
     add_seg(D.sic_ent, sic.ent.size() * 4, sic.ent.data());
     add_seg(D.fac, S * std::max<std::size_t>(a8, 8), nullptr);
+    add_seg(D.fac_any, (S + 1) * 4, nullptr);
     add_seg(D.sic_part,
             2 * static_cast<std::size_t>(std::max(D.sic_parts - 1, 1)) * D.sic_npad * 8, nullptr);
     add_seg(D.sic_val, static_cast<std::size_t>(D.sic_ring) * std::max<std::size_t>(n8, 8), nullptr);

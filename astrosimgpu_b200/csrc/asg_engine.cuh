@@ -166,6 +166,11 @@ struct InstDev {
     const std::uint32_t* sic_soff;  // [P*sic_npad/32+1] entry offset of each 32-target slice
     const std::uint32_t* sic_ent;   // astro << 8 | mult
     double* fac;                    // [slots][NA]
+    // fac_any[e % (slots + 1)] != 0: some factor of emission step e is
+    // non-zero.  Set by the astrocyte role, cleared one step ahead by the
+    // instance's first astrocyte block; a fused SIC sum of an arrival whose
+    // emission had none is the +0.0 it would add up to, without its loads.
+    std::uint32_t* fac_any;         // [slots + 1]
     double* sic_part;               // [2][P-1][sic_npad] partial sums, by step parity
     double* sic_val;                // [sic_ring][N], slot = arrival step % sic_ring
     // outputs (host-mapped memory)

@@ -58,6 +58,9 @@ struct StepInfo {
     std::uint32_t rec_row;
     std::uint64_t noise_e, noise_i, noise_a;  // noise draw indices
     std::int32_t sic_now, fac_now, rec_now;
+    // fac_any indices: this step's emission, the next step's (cleared now),
+    // and the emission the fused SIC of this step reads (-1: none yet)
+    std::int32_t fany_now, fany_next, fany_read;
 };
 
 // Computed by warp 0 of the block: each lane forms one quotient and
@@ -82,6 +85,9 @@ __device__ void make_step_info(const InstDev& I, std::int64_t step, StepInfo& S)
     if (lane == 12) { d = I.a_steps_per_noise; }
     if (lane >= 13 && lane < 13 + P) { n = step + P - (lane - 13) - I.d_a2n; d = I.sic_interval; }
     if (lane >= 13 + P && lane < 13 + 2 * P) { n = step + P - (lane - 13 - P) - I.d_a2n; }
+    if (lane == 29) { d = I.slots + 1; }
+    if (lane == 30) { n = step + 1; d = I.slots + 1; }
+    if (lane == 31) { n = step - I.d_a2n; d = I.slots + 1; }
     std::int64_t q = -1, r = -1;  // -1: negative numerator (not yet due)
     if (n >= 0) {
         const auto un = static_cast<unsigned long long>(n), ud = static_cast<unsigned long long>(d);
@@ -117,6 +123,9 @@ __device__ void make_step_info(const InstDev& I, std::int64_t step, StepInfo& S)
         S.noise_e = static_cast<std::uint64_t>(s_q[10]);
         S.noise_i = static_cast<std::uint64_t>(s_q[11]);
         S.noise_a = static_cast<std::uint64_t>(s_q[12]);
+        S.fany_now = static_cast<std::int32_t>(s_r[29]);
+        S.fany_next = static_cast<std::int32_t>(s_r[30]);
+        S.fany_read = static_cast<std::int32_t>(s_r[31]);
     }
 }
 
@@ -567,7 +576,10 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
             if (in != 0.0) add_syn(-in, exc_in, inh_in);
         }
         if (sic_due) {
-            if (I.fused_sic) Isic = fused_sic(I, c, S.fslot);
+            if (I.fused_sic)
+                Isic = (S.fany_read >= 0 && __ldcg(I.fac_any + S.fany_read) != 0u)
+                           ? fused_sic(I, c, S.fslot)
+                           : 0.0;  // no emitting astrocyte: the sum of no terms
             I.Isic[c] = Isic;
         }
 
@@ -903,6 +915,9 @@ __device__ void astro_role(const InstDev& I, const StepInfo& S, const Work& wk) 
     }
     if (kPdl) grid_dep_wait();
     const std::int64_t step = S.step;
+    // The next step's emission flag starts clear (nothing reads or writes
+    // that entry during this step: see InstDev::fac_any).
+    if (wk.first == 0 && threadIdx.x == 0 && step < I.end_step) I.fac_any[S.fany_next] = 0u;
     if (!active || step >= I.end_step) return;
     const std::uint32_t slot = S.slot;
     const std::size_t ts = static_cast<std::size_t>(slot) * I.ring_as.n_targets + a;
@@ -941,7 +956,9 @@ __device__ void astro_role(const InstDev& I, const StepInfo& S, const Work& wk) 
     // of the arrival step.
     if (S.fac_now) {
         const double y = (ca - I.SIC_th) * 1000.0;
-        I.fac[static_cast<std::size_t>(slot) * I.NA + a] = y <= 1.0 ? 0.0 : I.SIC_scale * log(y);
+        const double f = y <= 1.0 ? 0.0 : I.SIC_scale * log(y);
+        I.fac[static_cast<std::size_t>(slot) * I.NA + a] = f;
+        if (f != 0.0) I.fac_any[S.fany_now] = 1u;  // every writer stores the same 1
     }
     if (I.rec_astro_max > 0 && a < I.rec_astro_max && S.rec_now) {
         const std::size_t row = S.rec_row;
