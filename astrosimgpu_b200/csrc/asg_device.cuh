@@ -142,7 +142,9 @@ static __device__ __noinline__ int poisson_large(std::uint64_t seed, std::uint64
 // against IEEE division over random and edge-case operands of every class.
 __host__ __device__ __noinline__ inline double ieee_div(double a, double b) { return a / b; }
 
-__host__ __device__ __forceinline__ double div_by(double a, double b, double y) {
+// Numerator outside the range where the reciprocal division is exact
+// without a test (div_by's exponent test, as an integer flag).
+__host__ __device__ __forceinline__ unsigned div_out_of_range(double a) {
 #ifdef __CUDA_ARCH__
     const unsigned biased = (static_cast<unsigned>(__double2hiint(a)) >> 20) & 0x7FFu;
 #else
@@ -150,10 +152,21 @@ __host__ __device__ __forceinline__ double div_by(double a, double b, double y) 
     __builtin_memcpy(&u, &a, sizeof u);
     const unsigned biased = static_cast<unsigned>(u >> 52) & 0x7FFu;
 #endif
-    if (biased - 64u > 1936u) return ieee_div(a, b);  // biased exponent outside [64, 2000]
+    return (biased - 64u > 1936u) ? 1u : 0u;
+}
+
+// div_by without its exponent test, for callers that test the numerator
+// themselves (div_out_of_range) and redo the case it flags.
+__host__ __device__ __forceinline__ double div_by_untested(double a, double b, double y) {
     const double q = a * y;
     const double r = fma(-q, b, a);
     return fma(r, y, q);
+}
+
+__host__ __device__ __forceinline__ double div_by(double a, double b, double y) {
+    // biased exponent outside [64, 2000]: the IEEE division itself
+    if (div_out_of_range(a)) return ieee_div(a, b);
+    return div_by_untested(a, b, y);
 }
 
 
@@ -396,21 +409,55 @@ struct AdexRates {
 // `with_spike` is false: the refractory branch of the reference evaluates it
 // but only uses dw, which does not depend on it.
 template <bool with_spike>
+__device__ __noinline__ AdexRates adex_ieee(const NeuronK& p, double V, double w, double g_ex,
+                                            double g_in, double I_ext);
+
+template <bool with_spike>
 __device__ __forceinline__ AdexRates adex(const NeuronK& p, double V, double w, double g_ex,
                                           double g_in, double I_ext) {
     const double v = (p.V_peak < V) ? p.V_peak : V;  // std::min(V, V_peak)
     const double rel = v - p.E_L;
     AdexRates r;
+    // The three divisions go through the reciprocals untested; their
+    // numerators' exponent tests are or-ed into one flag (integer work off
+    // the FP64 chain), and the rare evaluation they flag is redone with IEEE
+    // divisions: one branch per right-hand side instead of one per division.
+    unsigned bad = 0u;
     if (with_spike) {
-        const double spike = p.gl_dt * exp(div_by(v - p.V_th, p.Delta_T, p.inv_Delta_T));
+        const double n_spike = v - p.V_th;
+        bad |= div_out_of_range(n_spike);
+        const double spike = p.gl_dt * exp(div_by_untested(n_spike, p.Delta_T, p.inv_Delta_T));
         const double syn_ex = g_ex * (v - p.E_ex);
         const double syn_in = g_in * (v - p.E_in);
-        r.V = div_by(p.neg_g_L * rel + spike - syn_ex - syn_in - w + p.I_e + I_ext, p.C_m,
-                     p.inv_C_m);
+        const double n_V = p.neg_g_L * rel + spike - syn_ex - syn_in - w + p.I_e + I_ext;
+        bad |= div_out_of_range(n_V);
+        r.V = div_by_untested(n_V, p.C_m, p.inv_C_m);
     } else {
         r.V = 0.0;
     }
-    r.w = div_by(p.a * rel - w, p.tau_w, p.inv_tau_w);
+    const double n_w = p.a * rel - w;
+    bad |= div_out_of_range(n_w);
+    r.w = div_by_untested(n_w, p.tau_w, p.inv_tau_w);
+    if (bad != 0u) r = adex_ieee<with_spike>(p, V, w, g_ex, g_in, I_ext);
+    return r;
+}
+
+// The same right-hand side with IEEE divisions (out of line: the rare case).
+template <bool with_spike>
+__device__ __noinline__ AdexRates adex_ieee(const NeuronK& p, double V, double w, double g_ex,
+                                            double g_in, double I_ext) {
+    const double v = (p.V_peak < V) ? p.V_peak : V;
+    const double rel = v - p.E_L;
+    AdexRates r;
+    if (with_spike) {
+        const double spike = p.gl_dt * exp((v - p.V_th) / p.Delta_T);
+        const double syn_ex = g_ex * (v - p.E_ex);
+        const double syn_in = g_in * (v - p.E_in);
+        r.V = (p.neg_g_L * rel + spike - syn_ex - syn_in - w + p.I_e + I_ext) / p.C_m;
+    } else {
+        r.V = 0.0;
+    }
+    r.w = (p.a * rel - w) / p.tau_w;
     return r;
 }
 
