@@ -1069,7 +1069,8 @@ cudaError_t Engine::issue_steps(int steps) {
             e = cudaStreamWaitEvent(stream, ev_side_done[((k - side_lead) / G) % kSideEvents], 0);
         if (e == cudaSuccess)
             e = launch_step(d_insts.as<InstDev>(), d_work.as<Work>(), static_cast<int>(work.size()),
-                            cfg.block, k, cfg.pdl && k > 0, wide, wide_grid, stream);
+                            cfg.block, k, cfg.pdl && k > 0, wide, wide_grid, cfg.astro_fp32,
+                            stream);
     }
     if (side_on && e == cudaSuccess) {
         e = cudaEventRecord(ev_side_join, side);
@@ -1128,7 +1129,7 @@ int Engine::launch_chunk(int parity, int steps) {
         ASG_CUDA(launch_chunk_persistent(d_insts.as<InstDev>(), d_work.as<Work>(),
                                          static_cast<int>(work.size()), cfg.block,
                                          persistent_grid, steps, d_barrier.as<GridBarrier>(),
-                                         stream));
+                                         cfg.astro_fp32, stream));
         ASG_CUDA(cudaMemcpyAsync(h_barrier_err[parity], &d_barrier.as<GridBarrier>()->error,
                                  sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
     } else if (cudaGraphExec_t g = graph_mode() ? find_graph(steps) : nullptr) {

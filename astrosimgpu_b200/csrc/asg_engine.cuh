@@ -198,7 +198,7 @@ cudaError_t barrier_selftest(GridBarrier* gb, cudaStream_t stream);
 int persistent_blocks(int block);
 // All `steps` steps of a chunk in one cooperative launch of `grid` blocks.
 cudaError_t launch_chunk_persistent(const InstDev* insts, const Work* work, int n_work,
-                                    int block, int grid, int steps, GridBarrier* gb,
+                                    int block, int grid, int steps, GridBarrier* gb, bool f32,
                                     cudaStream_t stream);
 
 // One side-stream SIC batch (instances with sic_side): the arrival steps
@@ -213,7 +213,7 @@ cudaError_t launch_sic_batch(const InstDev* insts, const Work* work, int n_work,
 // One step launch over the work table.  max_grid > 0 caps the grid (blocks
 // then run several work items each); 0 launches one block per item.
 cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
-                        bool pdl, bool wide, int max_grid, cudaStream_t stream);
+                        bool pdl, bool wide, int max_grid, bool f32, cudaStream_t stream);
 // Resident blocks per SM of the high-occupancy step kernel form (128 threads).
 int step_wide_blocks_per_sm();
 

@@ -694,8 +694,7 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
         const unsigned wbase = threadIdx.x & ~31u;
         const unsigned left = wk.count - wbase;  // > 0 for an active lane
         const unsigned act = left >= 32u ? 0xFFFFFFFFu : ((1u << left) - 1u);
-        __syncwarp(act);
-        const unsigned smask = __ballot_sync(act, spiked);
+        const unsigned smask = __ballot_sync(act, spiked);  // synchronises the lanes of act
         if (smask != 0u) {
             const unsigned rank = __popc(smask & ((1u << lane) - 1u));
             const int leader = __ffs(smask) - 1;
@@ -900,7 +899,7 @@ __device__ __noinline__ void astro_update_f32(const InstDev& I, double ca_tot, d
     hh = hv;
 }
 
-template <bool kPdl>
+template <bool kPdl, bool kF32>
 __device__ void astro_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     const std::uint32_t a = wk.first + threadIdx.x;
     const bool active = threadIdx.x < wk.count;
@@ -945,7 +944,9 @@ __device__ void astro_role(const InstDev& I, const StepInfo& S, const Work& wk) 
     }
     if (ev > 0) ip3_in += I.a_weight * static_cast<double>(ev);
     // AstrocytePopulation::update (astrocyte.cpp:307-329)
-    if (I.astro_fp32)
+    // (the precision study's FP32 form is a separate instantiation: the FP64
+    // kernels carry none of its code)
+    if constexpr (kF32)
         astro_update_f32(I, ca_tot, ip3_0, tau, delta, ip3_in, noise, ca, ip3, hh);
     else
         astro_rk4<false>(I.ak, ca_tot, ip3_0, tau, inv_tau, delta, ip3_in, noise, ca, ip3, hh);
@@ -1009,7 +1010,7 @@ __device__ void sic_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     if ((threadIdx.x & 31) == 0 && edges) atomicAdd(I.counters + 1, edges);
 }
 
-template <bool kPdl>
+template <bool kPdl, bool kF32>
 __device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     if (wk.role == kRolePush) {
         push_role<kPdl>(I, S, wk);
@@ -1018,7 +1019,7 @@ __device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, co
     if (wk.role == kRoleNeuron) {
         neuron_role<kPdl>(I, S, wk);
     } else if (wk.role == kRoleAstro) {
-        astro_role<kPdl>(I, S, wk);
+        astro_role<kPdl, kF32>(I, S, wk);
     } else {
         sic_role<kPdl>(I, S, wk);
     }
@@ -1031,6 +1032,7 @@ __device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, co
 // is one wave of resident blocks (a large step), which saves the per-block
 // staging and scheduling of the items after the first.  No item waits on
 // another within a launch, so any assignment of items to blocks is valid.
+template <bool kF32>
 __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
                                           const Work* __restrict__ work, int k, int n_work) {
     // Stage the item's instance descriptor and step arithmetic in shared
@@ -1063,7 +1065,7 @@ __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
             }
             staged = wk.inst;
         }
-        run_role<true>(I, s_info, wk);
+        run_role<true, kF32>(I, s_info, wk);
         __syncthreads();  // the role's shared arrays are free for the next item
     }
 }
@@ -1074,16 +1076,18 @@ __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
 // waves); step_kernel_wide is for 128-thread blocks at 6 per SM (80
 // registers, some spilled: more warps to hide latency when a step is many
 // waves of blocks).
+template <bool kF32>
 __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restrict__ insts,
                                                          const Work* __restrict__ work, int k,
                                                          int n_work) {
-    step_body(insts, work, k, n_work);
+    step_body<kF32>(insts, work, k, n_work);
 }
 
+template <bool kF32>
 __global__ void __launch_bounds__(128, 6) step_kernel_wide(const InstDev* __restrict__ insts,
                                                            const Work* __restrict__ work, int k,
                                                            int n_work) {
-    step_body(insts, work, k, n_work);
+    step_body<kF32>(insts, work, k, n_work);
 }
 
 // Grid-wide barrier of the persistent chunk kernel (all blocks co-resident
@@ -1145,6 +1149,7 @@ __device__ bool grid_sync(GridBarrier* gb, unsigned nblocks) {
 // work items blockIdx.x, blockIdx.x + gridDim.x, ... of every step, with a
 // grid barrier between steps.  Data other blocks wrote in earlier steps is
 // read through L2 (__ldcg in the roles), never a stale L1 line.
+template <bool kF32>
 __global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restrict__ insts,
                                                           const Work* __restrict__ work,
                                                           int n_work, int steps,
@@ -1168,7 +1173,7 @@ __global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restr
             }
             if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
             __syncthreads();
-            if (s_info.step < I.end_step) run_role<false>(I, s_info, wk);
+            if (s_info.step < I.end_step) run_role<false, kF32>(I, s_info, wk);
         }
         if (k + 1 < steps && !grid_sync(gb, gridDim.x)) return;
     }
@@ -1275,7 +1280,7 @@ cudaError_t barrier_selftest(GridBarrier* gb, cudaStream_t stream) {
 
 int persistent_blocks(int block) {
     int per_sm = 0, dev = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chunk_kernel, block, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chunk_kernel<false>, block, 0) !=
         cudaSuccess)
         return 0;
     cudaGetDevice(&dev);
@@ -1284,7 +1289,7 @@ int persistent_blocks(int block) {
 }
 
 cudaError_t launch_chunk_persistent(const InstDev* insts, const Work* work, int n_work,
-                                    int block, int grid, int steps, GridBarrier* gb,
+                                    int block, int grid, int steps, GridBarrier* gb, bool f32,
                                     cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(static_cast<unsigned>(grid));
@@ -1296,18 +1301,20 @@ cudaError_t launch_chunk_persistent(const InstDev* insts, const Work* work, int 
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, chunk_kernel, insts, work, n_work, steps, gb);
+    if (f32) return cudaLaunchKernelEx(&cfg, chunk_kernel<true>, insts, work, n_work, steps, gb);
+    return cudaLaunchKernelEx(&cfg, chunk_kernel<false>, insts, work, n_work, steps, gb);
 }
 
 int step_wide_blocks_per_sm() {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step_kernel_wide, 128, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step_kernel_wide<false>, 128, 0) !=
+        cudaSuccess)
         return 0;
     return nb;
 }
 
 cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int block, int k,
-                        bool pdl, bool wide, int max_grid, cudaStream_t stream) {
+                        bool pdl, bool wide, int max_grid, bool f32, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(static_cast<unsigned>(max_grid > 0 ? std::min(n_work, max_grid) : n_work));
     cfg.blockDim = dim3(static_cast<unsigned>(block));
@@ -1319,8 +1326,10 @@ cudaError_t launch_step(const InstDev* insts, const Work* work, int n_work, int 
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     if (wide && block == 128)
-        return cudaLaunchKernelEx(&cfg, step_kernel_wide, insts, work, k, n_work);
-    return cudaLaunchKernelEx(&cfg, step_kernel, insts, work, k, n_work);
+        return f32 ? cudaLaunchKernelEx(&cfg, step_kernel_wide<true>, insts, work, k, n_work)
+                   : cudaLaunchKernelEx(&cfg, step_kernel_wide<false>, insts, work, k, n_work);
+    return f32 ? cudaLaunchKernelEx(&cfg, step_kernel<true>, insts, work, k, n_work)
+               : cudaLaunchKernelEx(&cfg, step_kernel<false>, insts, work, k, n_work);
 }
 
 }  // namespace asg
