@@ -3,11 +3,15 @@ checkpoint and resume.
 
     python -m astrosimgpu_b200.run --config paper_sparse_dt005 --steps 16000 --save ck.bin
     python -m astrosimgpu_b200.run --config paper_sparse_dt005 --load ck.bin --steps 8 --plain
+    python -m astrosimgpu_b200.run --serving 1000000 --steps 120 --plain
 
 A checkpoint is the engine's device state of one network (asg_checkpoint):
 resuming it in a network built from the same configuration continues the
 run bit for bit.  `--plain` launches one kernel per step without CUDA graphs
-(each launch then shows up on its own in a profiler).
+(each launch then shows up on its own in a profiler).  `--serving N` runs the
+serving-shaped network of N neurons and N astrocytes instead (use_case
+parameters, fixed in-degree 100, generated on the device), the shape of the
+largest request of the serving stream.
 """
 from __future__ import annotations
 
@@ -26,6 +30,9 @@ def main(argv=None) -> int:
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--config", default="paper_sparse_dt005",
                     help="shipped configuration name or path to a JSON file")
+    ap.add_argument("--serving", type=int, default=0,
+                    help="run the serving-shaped network of this many neurons instead")
+    ap.add_argument("--seed", type=int, default=99, help="seed of the --serving network")
     ap.add_argument("--steps", type=int, required=True)
     ap.add_argument("--save", help="write a checkpoint after the steps")
     ap.add_argument("--load", help="resume from a checkpoint before the steps")
@@ -34,8 +41,14 @@ def main(argv=None) -> int:
                     help="steps per chunk (0: the engine's default for the network size)")
     args = ap.parse_args(argv)
 
-    path = args.config if os.path.exists(args.config) else config_path(args.config)
-    model = Model(path, pre_time=0.0)
+    if args.serving:
+        from .workloads import serving_config
+        model = Model(text=serving_config(args.serving, args.seed, 100.0), pre_time=0.0,
+                      fixed_indegree=100, gen_device=0)
+        args.config = f"serving {args.serving} neurons, seed {args.seed}"
+    else:
+        path = args.config if os.path.exists(args.config) else config_path(args.config)
+        model = Model(path, pre_time=0.0)
     opts = dict(chunk_steps=args.chunk)
     if args.plain:
         opts["use_graphs"] = -1
