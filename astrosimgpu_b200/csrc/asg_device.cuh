@@ -408,20 +408,21 @@ struct AdexRates {
 // AdEx membrane and adaptation rates.  The spike current is skipped when
 // `with_spike` is false: the refractory branch of the reference evaluates it
 // but only uses dw, which does not depend on it.
-//
-// The three divisions go through the reciprocals untested; their numerators'
-// exponent tests are or-ed into `bad` (integer work off the FP64 chain).  A
-// caller that finds `bad` set after a whole RK4 substep redoes that substep
-// from its start with IEEE divisions (adex_substep_ieee): while `bad` stays
-// clear every division was exact, so the result is the reference's either
-// way, and the fast path carries one branch per substep.
 template <bool with_spike>
-__device__ __forceinline__ AdexRates adex_flagged(const NeuronK& p, double V, double w,
-                                                  double g_ex, double g_in, double I_ext,
-                                                  unsigned& bad) {
+__device__ __noinline__ AdexRates adex_ieee(const NeuronK& p, double V, double w, double g_ex,
+                                            double g_in, double I_ext);
+
+template <bool with_spike>
+__device__ __forceinline__ AdexRates adex(const NeuronK& p, double V, double w, double g_ex,
+                                          double g_in, double I_ext) {
     const double v = (p.V_peak < V) ? p.V_peak : V;  // std::min(V, V_peak)
     const double rel = v - p.E_L;
     AdexRates r;
+    // The three divisions go through the reciprocals untested; their
+    // numerators' exponent tests are or-ed into one flag (integer work off
+    // the FP64 chain), and the rare evaluation they flag is redone with IEEE
+    // divisions: one branch per right-hand side instead of one per division.
+    unsigned bad = 0u;
     if (with_spike) {
         const double n_spike = v - p.V_th;
         bad |= div_out_of_range(n_spike);
@@ -437,13 +438,14 @@ __device__ __forceinline__ AdexRates adex_flagged(const NeuronK& p, double V, do
     const double n_w = p.a * rel - w;
     bad |= div_out_of_range(n_w);
     r.w = div_by_untested(n_w, p.tau_w, p.inv_tau_w);
+    if (bad != 0u) r = adex_ieee<with_spike>(p, V, w, g_ex, g_in, I_ext);
     return r;
 }
 
-// The same right-hand side with IEEE divisions.
+// The same right-hand side with IEEE divisions (out of line: the rare case).
 template <bool with_spike>
-__device__ __forceinline__ AdexRates adex_ieee(const NeuronK& p, double V, double w,
-                                               double g_ex, double g_in, double I_ext) {
+__device__ __noinline__ AdexRates adex_ieee(const NeuronK& p, double V, double w, double g_ex,
+                                            double g_in, double I_ext) {
     const double v = (p.V_peak < V) ? p.V_peak : V;
     const double rel = v - p.E_L;
     AdexRates r;
@@ -457,58 +459,6 @@ __device__ __forceinline__ AdexRates adex_ieee(const NeuronK& p, double V, doubl
     }
     r.w = (p.a * rel - w) / p.tau_w;
     return r;
-}
-
-// Conductances of one substep: at its start (stage 1), midpoint (stages 2, 3)
-// and end (stage 4).
-struct SubstepG {
-    double ex0, in0, exm, inm, ex1, in1;
-};
-
-// One RK4 substep of (V, w) (neuron.cpp:285-298), the stages as a loop; the
-// stage sum k1 + 2 k2 + 2 k3 + k4 accumulates left to right.  kIeee selects
-// the IEEE divisions (the redo of a flagged substep, out of line).
-template <bool kIeee>
-__device__ __forceinline__ AdexRates adex_rk4_substep(const NeuronK& p, double V, double w,
-                                                      const SubstepG& g, double I_ext,
-                                                      double h, double half_h, double h6,
-                                                      unsigned& bad) {
-    double sV = 0.0, sw = 0.0, xV = V, xw = w;
-#pragma unroll 1
-    for (int stg = 0; stg < 4; ++stg) {
-        const double ge = stg == 0 ? g.ex0 : (stg < 3 ? g.exm : g.ex1);
-        const double gi = stg == 0 ? g.in0 : (stg < 3 ? g.inm : g.in1);
-        const AdexRates r = kIeee ? adex_ieee<true>(p, xV, xw, ge, gi, I_ext)
-                                  : adex_flagged<true>(p, xV, xw, ge, gi, I_ext, bad);
-        if (stg == 0) {
-            sV = r.V;
-            sw = r.w;
-        } else if (stg < 3) {
-            sV = fma(2.0, r.V, sV);  // = sV + 2.0 * r.V: 2r is exact
-            sw = fma(2.0, r.w, sw);
-        } else {
-            sV = sV + r.V;
-            sw = sw + r.w;
-        }
-        const double stp = stg < 2 ? half_h : h;
-        xV = V + stp * r.V;
-        xw = w + stp * r.w;
-    }
-    return AdexRates{V + h6 * sV, w + h6 * sw};
-}
-
-__device__ __noinline__ inline AdexRates adex_rk4_substep_ieee(const NeuronK& p, double V, double w,
-                                                        SubstepG g, double I_ext, double h,
-                                                        double half_h, double h6) {
-    unsigned unused = 0u;
-    return adex_rk4_substep<true>(p, V, w, g, I_ext, h, half_h, h6, unused);
-}
-
-// The refractory substep's w update, w + h * dw, with IEEE divisions.
-__device__ __noinline__ inline double adex_refractory_w_ieee(const NeuronK& p, double V, double w,
-                                                      double g_ex, double g_in, double I_ext,
-                                                      double h) {
-    return w + h * adex_ieee<false>(p, V, w, g_ex, g_in, I_ext).w;
 }
 
 }  // namespace asg

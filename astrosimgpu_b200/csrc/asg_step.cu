@@ -601,19 +601,35 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
             const double dgin1 = P.decay_in * dgin;
             if (refr > 0) {
                 V = Vr;
-                unsigned bad = 0u;
-                const AdexRates r = adex_flagged<false>(P, V, w, gex, gin, Iext, bad);
-                w = bad ? adex_refractory_w_ieee(P, V, w, gex, gin, Iext, h) : w + h * r.w;
+                const AdexRates r = adex<false>(P, V, w, gex, gin, Iext);
+                w += h * r.w;
             } else {
                 // RK4 with the conductances at the start, midpoint and end of
-                // the substep; a substep whose divisions left the exact range
-                // is redone with IEEE divisions.
-                const SubstepG g{gex, gin, 0.5 * (gex + gex1), 0.5 * (gin + gin1), gex1, gin1};
-                unsigned bad = 0u;
-                AdexRates nx = adex_rk4_substep<false>(P, V, w, g, Iext, h, half_h, h6, bad);
-                if (bad) nx = adex_rk4_substep_ieee(P, V, w, g, Iext, h, half_h, h6);
-                V = nx.V;
-                w = nx.w;
+                // the substep (neuron.cpp:285-298), stages as a loop; the stage
+                // sum k1 + 2 k2 + 2 k3 + k4 accumulates left to right.
+                const double gexm = 0.5 * (gex + gex1), ginm = 0.5 * (gin + gin1);
+                double sV = 0.0, sw = 0.0, xV = V, xw = w;
+#pragma unroll 1
+                for (int stg = 0; stg < 4; ++stg) {
+                    const double ge = stg == 0 ? gex : (stg < 3 ? gexm : gex1);
+                    const double gi = stg == 0 ? gin : (stg < 3 ? ginm : gin1);
+                    const AdexRates r = adex<true>(P, xV, xw, ge, gi, Iext);
+                    if (stg == 0) {
+                        sV = r.V;
+                        sw = r.w;
+                    } else if (stg < 3) {
+                        sV = fma(2.0, r.V, sV);  // = sV + 2.0 * r.V: 2r is exact
+                        sw = fma(2.0, r.w, sw);
+                    } else {
+                        sV = sV + r.V;
+                        sw = sw + r.w;
+                    }
+                    const double stp = stg < 2 ? half_h : h;
+                    xV = V + stp * r.V;
+                    xw = w + stp * r.w;
+                }
+                V += h6 * sV;
+                w += h6 * sw;
             }
             gex = gex1;
             dgex = dgex1;
