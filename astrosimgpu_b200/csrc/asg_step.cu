@@ -1201,9 +1201,8 @@ __global__ void __launch_bounds__(kMaxBlock) sic_batch_kernel(const InstDev* __r
         std::uint32_t o0 = 0, len = 0, e[kSicBatch];
         sic_prefetch(I, t, o0, len, e);
         const double* fac[G];
-        bool due[G], emits[G];
+        bool due[G];
         double acc[G];
-        bool any = false;
 #pragma unroll
         for (int j = 0; j < G; ++j) {
             const std::int64_t a = I.step0 + k + I.sic_lead + j;
@@ -1211,14 +1210,8 @@ __global__ void __launch_bounds__(kMaxBlock) sic_batch_kernel(const InstDev* __r
             due[j] = a >= I.step0 && se >= 0 && se % I.sic_interval == 0;
             fac[j] = I.fac + static_cast<std::size_t>(due[j] ? se % I.slots : 0) * I.NA;
             acc[j] = 0.0;
-            // An emission step with no astrocyte above threshold adds only
-            // +0.0 terms: its factors need not be read (InstDev::fac_any;
-            // the emissions precede this batch and their flags are cleared
-            // only after its readers ran).
-            emits[j] = due[j] && __ldcg(I.fac_any + se % (I.slots + 1)) != 0u;
-            any = any || emits[j];
         }
-        for (std::uint32_t b0 = 0; any; b0 += kSicBatch) {
+        for (std::uint32_t b0 = 0;; b0 += kSicBatch) {
             bool done = false;
             for (int q = 0; q < kSicBatch; ++q) {
                 const std::uint32_t m = e[q] & 0xFFu;
@@ -1230,7 +1223,7 @@ __global__ void __launch_bounds__(kMaxBlock) sic_batch_kernel(const InstDev* __r
                 double c[G];
 #pragma unroll
                 for (int j = 0; j < G; ++j) {
-                    const double f = emits[j] ? __ldcg(fac[j] + as) : 0.0;
+                    const double f = __ldcg(fac[j] + as);
                     c[j] = I.w_a2n * f;
                     if (due[j] && f != 0.0) edges += m;
                     if (f == 0.0) c[j] = 0.0;
