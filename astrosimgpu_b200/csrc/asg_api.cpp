@@ -329,6 +329,7 @@ int asg_restore(asg_network* net, const void* host_buf, uint64_t bytes) {
     ASG_CUDA(cudaMemcpy(I->arena.get(), static_cast<const char*>(host_buf) + 8, I->arena_bytes,
                         cudaMemcpyHostToDevice));
     I->spikes.clear();
+    I->dev.noise_from = I->step;  // noise terms drawn afresh at the first step
     h->eng->mark_side_prime();
     return ASG_OK;
 }

@@ -767,6 +767,8 @@ int Engine::prepare(const asg_network_desc& d, const asg_record_opts* rec, std::
     add_seg(D.sic_ent, sic.ent.size() * 4, sic.ent.data());
     add_seg(D.fac, S * std::max<std::size_t>(a8, 8), nullptr);
     add_seg(D.fac_any, (S + 1) * 4, nullptr);
+    add_seg(D.noise_n, n8, nullptr);
+    add_seg(D.noise_a, a8, nullptr);
     add_seg(D.sic_part,
             2 * static_cast<std::size_t>(std::max(D.sic_parts - 1, 1)) * D.sic_npad * 8, nullptr);
     add_seg(D.sic_val, static_cast<std::size_t>(D.sic_ring) * std::max<std::size_t>(n8, 8), nullptr);
@@ -828,6 +830,7 @@ int Engine::prepare(const asg_network_desc& d, const asg_record_opts* rec, std::
         ASG_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&I.rec_d[p]), I.rec_h[p], 0));
     }
     D.spike_log_cap = D.rec_spikes ? I.log_cap : 0;
+    D.noise_from = first;  // the noise-term caches hold nothing yet
     I.step = first;
     I.end = end;
     *out = std::move(inst);

@@ -116,6 +116,14 @@ struct InstDev {
     double Ca_tot_u, IP3_0_u, tau_u, delta_u, inv_tau_u;
     double a_rate, a_weight, a_lambda, a_limit, a_std;
     std::int32_t a_indep, a_steps_per_noise;
+    // Noise terms of the current noise interval: a draw index changes every
+    // steps_per_noise steps, and between changes the term is read back here
+    // instead of drawn again (the same bits: the draw depends only on seed,
+    // index and cell).  Drawn afresh at each interval's first step and at
+    // noise_from, the first step after the instance was created or restored.
+    double* noise_n;  // [N]  noise_std * z of each neuron
+    double* noise_a;  // [NA] a_std * z of each astrocyte
+    std::int64_t noise_from;
     double SIC_scale, SIC_th;
     // synapses
     double w_e, w_i, w_n2a, w_a2n, U, tau_rec, tau_fac;

@@ -58,6 +58,8 @@ struct StepInfo {
     std::uint32_t rec_row;
     std::uint64_t noise_e, noise_i, noise_a;  // noise draw indices
     std::int32_t sic_now, fac_now, rec_now;
+    // noise terms drawn this step (else read from the cache): exc, inh, astro
+    std::int32_t fresh_e, fresh_i, fresh_a;
     // fac_any indices: this step's emission, the next step's (cleared now),
     // and the emission the fused SIC of this step reads (-1: none yet)
     std::int32_t fany_now, fany_next, fany_read;
@@ -123,6 +125,10 @@ __device__ void make_step_info(const InstDev& I, std::int64_t step, StepInfo& S)
         S.noise_e = static_cast<std::uint64_t>(s_q[10]);
         S.noise_i = static_cast<std::uint64_t>(s_q[11]);
         S.noise_a = static_cast<std::uint64_t>(s_q[12]);
+        const bool restart = step == I.noise_from;
+        S.fresh_e = s_r[10] == 0 || restart;
+        S.fresh_i = s_r[11] == 0 || restart;
+        S.fresh_a = s_r[12] == 0 || restart;
         S.fany_now = static_cast<std::int32_t>(s_r[29]);
         S.fany_next = static_cast<std::int32_t>(s_r[30]);
         S.fany_read = static_cast<std::int32_t>(s_r[31]);
@@ -550,12 +556,21 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
                     static_cast<std::uint64_t>(step) * kStreamStride + c);
             ev = r.poisson(P.lambda, P.knuth_limit);
         }
-        double z = 0.0;
+        // Noise term noise_std * z (neuron.cpp:243-248), z drawn once per
+        // noise interval.
+        double zterm = 0.0;
         if (P.noise_std > 0.0) {
-            const std::uint64_t idx = exc ? S.noise_e : S.noise_i;
-            z = P.independent_noise
-                    ? normal_first_at(I.seed ^ kSaltNeuronNoise, idx * kNoiseStride + c)
-                    : normal_first_at(I.seed ^ (exc ? kSaltSharedExc : kSaltSharedInh), idx);
+            if (exc ? S.fresh_e : S.fresh_i) {
+                const std::uint64_t idx = exc ? S.noise_e : S.noise_i;
+                const double z =
+                    P.independent_noise
+                        ? normal_first_at(I.seed ^ kSaltNeuronNoise, idx * kNoiseStride + c)
+                        : normal_first_at(I.seed ^ (exc ? kSaltSharedExc : kSaltSharedInh), idx);
+                zterm = P.noise_std * z;
+                I.noise_n[c] = zterm;
+            } else {
+                zterm = I.noise_n[c];
+            }
         }
 
         // apply_arrivals (network.cpp:301-338): both short lists in one batch.
@@ -586,7 +601,7 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
         // Poisson drive and noise (neuron.cpp:228-248)
         if (ev > 0) exc_in += P.poiss_weight * static_cast<double>(ev);
         double Iext = Isic;
-        if (P.noise_std > 0.0) Iext += 0.0 + P.noise_std * z;
+        if (P.noise_std > 0.0) Iext += 0.0 + zterm;
 
         if (exc_in != 0.0) dgex += exc_in * P.psc_ex;
         if (inh_in != 0.0) dgin += inh_in * P.psc_in;
@@ -929,11 +944,16 @@ __device__ void astro_role(const InstDev& I, const StepInfo& S, const Work& wk) 
         Draws r(I.seed ^ kSaltAstroPoisson, static_cast<std::uint64_t>(step) * kStreamStride + a);
         ev = r.poisson(I.a_lambda, I.a_limit);
     }
-    double noise = 0.0;
+    double noise = 0.0;  // a_std * z, z drawn once per noise interval
     if (I.a_std > 0.0) {
-        const std::uint64_t nseed = I.seed ^ kSaltAstroNoise;
-        noise = I.a_std * normal_clamped_at(nseed, I.a_indep ? S.noise_a * kStreamStride + a
-                                                             : S.noise_a);
+        if (S.fresh_a) {
+            const std::uint64_t nseed = I.seed ^ kSaltAstroNoise;
+            noise = I.a_std * normal_clamped_at(nseed, I.a_indep ? S.noise_a * kStreamStride + a
+                                                                 : S.noise_a);
+            I.noise_a[a] = noise;
+        } else {
+            noise = I.noise_a[a];
+        }
     }
     double ip3_in = 0.0;
     if (n) {

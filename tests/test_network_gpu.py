@@ -326,9 +326,11 @@ def test_large_batch_fused_sic_equals_single_bitwise():
 
 
 def test_checkpoint_restore_bitwise():
+    """Resume inside a noise interval (step 503; the noise draws change every
+    10 steps), in the same network after it ran on and in a new one."""
     m = Model(config_path("use_case"), pre_time=0.0)
     n = Network(m, record=rec_all())
-    n.step(500)
+    n.step(503)
     blob = n.checkpoint()
     n.fetch_spikes()
     n.step(700)
@@ -336,9 +338,14 @@ def test_checkpoint_restore_bitwise():
     n.restore(blob)
     n.step(700)
     sp2, st2 = n.fetch_spikes(), n.state()
-    assert np.array_equal(sp1[0], sp2[0]) and np.array_equal(sp1[1], sp2[1])
-    for k in STATE_KEYS:
-        assert np.array_equal(st1[k], st2[k]), k
+    fresh = Network(m, record=rec_all())
+    fresh.restore(blob)
+    fresh.step(700)
+    sp3, st3 = fresh.fetch_spikes(), fresh.state()
+    for sp, st in ((sp2, st2), (sp3, st3)):
+        assert np.array_equal(sp1[0], sp[0]) and np.array_equal(sp1[1], sp[1])
+        for k in STATE_KEYS:
+            assert np.array_equal(st1[k], st[k]), k
 
 
 def test_recording_matches_reference_rows():
