@@ -620,11 +620,12 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
                 w += h * r.w;
             } else {
                 // RK4 with the conductances at the start, midpoint and end of
-                // the substep (neuron.cpp:285-298), stages as a loop; the stage
-                // sum k1 + 2 k2 + 2 k3 + k4 accumulates left to right.
+                // the substep (neuron.cpp:285-298), the four stages unrolled
+                // (no stage selects at run time); the stage sum
+                // k1 + 2 k2 + 2 k3 + k4 accumulates left to right.
                 const double gexm = 0.5 * (gex + gex1), ginm = 0.5 * (gin + gin1);
                 double sV = 0.0, sw = 0.0, xV = V, xw = w;
-#pragma unroll 1
+#pragma unroll
                 for (int stg = 0; stg < 4; ++stg) {
                     const double ge = stg == 0 ? gex : (stg < 3 ? gexm : gex1);
                     const double gi = stg == 0 ? gin : (stg < 3 ? ginm : gin1);
@@ -1047,12 +1048,13 @@ __device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, co
 }
 
 // One step of every resident instance (the body of both kernel forms below).
-// Block b runs work items b, b + gridDim.x, ...: one item per block when the
-// grid covers the work table (a step of a few waves), several when the grid
-// is one wave of resident blocks (a large step), which saves the per-block
-// staging and scheduling of the items after the first.  No item waits on
-// another within a launch, so any assignment of items to blocks is valid.
-template <bool kF32>
+// kLoop: block b runs work items b, b + gridDim.x, ... -- several when the
+// grid is one wave of resident blocks (a large step), which saves the
+// per-block staging and scheduling of the items after the first.  Without
+// kLoop the grid covers the work table and block b runs item b alone (a step
+// of a few waves: no loop structure on its path).  No item waits on another
+// within a launch, so any assignment of items to blocks is valid.
+template <bool kF32, bool kLoop>
 __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
                                           const Work* __restrict__ work, int k, int n_work) {
     // Stage the item's instance descriptor and step arithmetic in shared
@@ -1062,6 +1064,20 @@ __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
     __shared__ __align__(16) unsigned char s_raw[sizeof(InstDev)];
     __shared__ StepInfo s_info;
     const InstDev& I = *reinterpret_cast<const InstDev*>(s_raw);
+    if constexpr (!kLoop) {
+        const Work wk = load_work(work + blockIdx.x);  // gridDim.x == n_work
+        const auto* src = reinterpret_cast<const std::uint32_t*>(insts + wk.inst);
+        auto* dst = reinterpret_cast<std::uint32_t*>(s_raw);
+        for (unsigned i = threadIdx.x; i < sizeof(InstDev) / 4; i += blockDim.x)
+            dst[i] = __ldcg(src + i);
+        __syncthreads();
+        if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
+        __syncthreads();
+        asm volatile("griddepcontrol.launch_dependents;");  // see below
+        run_role<true, kF32>(I, s_info, wk);
+        (void)n_work;
+        return;
+    }
     std::uint32_t staged = 0xFFFFFFFFu;
     for (int wi = blockIdx.x; wi < n_work; wi += gridDim.x) {
         // Through L2 (never a cached line of an earlier chunk or engine):
@@ -1100,14 +1116,14 @@ template <bool kF32>
 __global__ void __launch_bounds__(kMaxBlock) step_kernel(const InstDev* __restrict__ insts,
                                                          const Work* __restrict__ work, int k,
                                                          int n_work) {
-    step_body<kF32>(insts, work, k, n_work);
+    step_body<kF32, false>(insts, work, k, n_work);
 }
 
 template <bool kF32>
 __global__ void __launch_bounds__(128, 6) step_kernel_wide(const InstDev* __restrict__ insts,
                                                            const Work* __restrict__ work, int k,
                                                            int n_work) {
-    step_body<kF32>(insts, work, k, n_work);
+    step_body<kF32, true>(insts, work, k, n_work);
 }
 
 // Grid-wide barrier of the persistent chunk kernel (all blocks co-resident
