@@ -490,7 +490,12 @@ __device__ __noinline__ double normal_clamped_at(std::uint64_t seed, std::uint64
 
 // --------------------------------------------------------------- roles
 
-template <bool kPdl>
+// kWarpAppend: a warp's spikes take one atomic per warp (ballot and prefix
+// sums), which pays off when a step has many spiking warps (the wide form);
+// otherwise each spiking thread appends itself, the shortest chain for the
+// few spikes of a small network's step.  Either order of the spike records
+// gives the same rings (the arrivals are summed in bit order).
+template <bool kPdl, bool kWarpAppend>
 __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     __shared__ std::uint32_t s_spk[kMaxBlock];
     __shared__ double s_val[2 * kMaxBlock];
@@ -699,6 +704,30 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
             }
         }
 
+        if constexpr (!kWarpAppend) {
+            if (spiked) {
+                // One atomic reserves this spike's record and edge range.
+                if (I.deferred_push) {
+                    const unsigned long long old = atomicAdd(
+                        I.spk_packed + S.ls * kHeaderStride,
+                        (1ull << 40) | static_cast<unsigned long long>(len0 + len1));
+                    const std::size_t o = static_cast<std::size_t>(S.ls) * I.N + (old >> 40);
+                    *reinterpret_cast<uint4*>(I.spk_meta + 4 * o) = make_uint4(
+                        r1, static_cast<std::uint32_t>(old & 0xFFFFFFFFFFull), r0, len0);
+                    *reinterpret_cast<double2*>(I.spk_val + 2 * o) = make_double2(v0, v1);
+                }
+                if (I.rec_spikes && step >= I.rec_from) {
+                    const unsigned long long li = atomicAdd(I.spike_log_n, 1ULL);
+                    if (li < I.spike_log_cap) {
+                        I.spike_log[li] = (static_cast<unsigned long long>(step) << 32) | c;
+                    } else {
+                        atomicAdd(I.counters + 3, 1ULL);
+                    }
+                }
+                atomicAdd(I.counters + 0, static_cast<unsigned long long>(len0 + len1));
+                atomicAdd(I.counters + 2, 1ULL);
+            }
+        }
         // The warp's spikes are compacted with a ballot and prefix sums: one
         // atomic per warp reserves the spike records and edge range of the
         // deferred push, one the spike-log entries, one each counter; every
@@ -710,8 +739,8 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
         const unsigned wbase = threadIdx.x & ~31u;
         const unsigned left = wk.count - wbase;  // > 0 for an active lane
         const unsigned act = left >= 32u ? 0xFFFFFFFFu : ((1u << left) - 1u);
-        const unsigned smask = __ballot_sync(act, spiked);  // synchronises the lanes of act
-        if (smask != 0u) {
+        const unsigned smask = kWarpAppend ? __ballot_sync(act, spiked) : 0u;  // syncs act
+        if (kWarpAppend && smask != 0u) {
             const unsigned rank = __popc(smask & ((1u << lane) - 1u));
             const int leader = __ffs(smask) - 1;
             const unsigned nspk = __popc(smask);
@@ -1031,14 +1060,14 @@ __device__ void sic_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     if ((threadIdx.x & 31) == 0 && edges) atomicAdd(I.counters + 1, edges);
 }
 
-template <bool kPdl, bool kF32>
+template <bool kPdl, bool kF32, bool kWarpAppend>
 __device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     if (wk.role == kRolePush) {
         push_role<kPdl>(I, S, wk);
         return;
     }
     if (wk.role == kRoleNeuron) {
-        neuron_role<kPdl>(I, S, wk);
+        neuron_role<kPdl, kWarpAppend>(I, S, wk);
     } else if (wk.role == kRoleAstro) {
         astro_role<kPdl, kF32>(I, S, wk);
     } else {
@@ -1074,7 +1103,7 @@ __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
         if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
         __syncthreads();
         asm volatile("griddepcontrol.launch_dependents;");  // see below
-        run_role<true, kF32>(I, s_info, wk);
+        run_role<true, kF32, false>(I, s_info, wk);
         (void)n_work;
         return;
     }
@@ -1101,7 +1130,7 @@ __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
             }
             staged = wk.inst;
         }
-        run_role<true, kF32>(I, s_info, wk);
+        run_role<true, kF32, true>(I, s_info, wk);
         __syncthreads();  // the role's shared arrays are free for the next item
     }
 }
@@ -1209,7 +1238,7 @@ __global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restr
             }
             if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
             __syncthreads();
-            if (s_info.step < I.end_step) run_role<false, kF32>(I, s_info, wk);
+            if (s_info.step < I.end_step) run_role<false, kF32, false>(I, s_info, wk);
         }
         if (k + 1 < steps && !grid_sync(gb, gridDim.x)) return;
     }
