@@ -920,12 +920,19 @@ __device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
 }
 
 // A non-push block's share of a burst push, after its own role.
-__device__ __noinline__ void help_push(const InstDev& I, const StepInfo& S, const Work& wk) {
-    if (!I.deferred_push || wk.helper == kNoHelper || S.step == 0 || S.step >= I.end_step) return;
+// `burst` carries the answer across the items a block runs in one step of
+// one instance (-1: not known yet, else 0 or 1), so the spike count is read
+// once per block rather than once per item; the new answer is returned.
+__device__ __noinline__ int help_push(const InstDev& I, const StepInfo& S, const Work& wk,
+                                      int burst) {
+    if (burst == 0 || !I.deferred_push || wk.helper == kNoHelper || S.step == 0 ||
+        S.step >= I.end_step)
+        return burst;
     const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev * kHeaderStride);
-    if (!push_burst(I, packed)) return;
+    if (!push_burst(I, packed)) return 0;
     push_spikes(I, S, packed, static_cast<std::uint32_t>(I.push_blocks) + wk.helper,
                 static_cast<std::uint32_t>(I.push_blocks + I.push_helpers));
+    return 1;
 }
 
 // The precision study's astrocyte update (astro_rk4_f32): state, parameters
@@ -1061,10 +1068,11 @@ __device__ void sic_role(const InstDev& I, const StepInfo& S, const Work& wk) {
 }
 
 template <bool kPdl, bool kF32, bool kWarpAppend>
-__device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, const Work& wk) {
+__device__ __forceinline__ int run_role(const InstDev& I, const StepInfo& S, const Work& wk,
+                                        int burst) {
     if (wk.role == kRolePush) {
         push_role<kPdl>(I, S, wk);
-        return;
+        return burst;
     }
     if (wk.role == kRoleNeuron) {
         neuron_role<kPdl, kWarpAppend>(I, S, wk);
@@ -1073,7 +1081,7 @@ __device__ __forceinline__ void run_role(const InstDev& I, const StepInfo& S, co
     } else {
         sic_role<kPdl>(I, S, wk);
     }
-    help_push(I, S, wk);
+    return help_push(I, S, wk, burst);
 }
 
 // One step of every resident instance (the body of both kernel forms below).
@@ -1103,11 +1111,12 @@ __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
         if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
         __syncthreads();
         asm volatile("griddepcontrol.launch_dependents;");  // see below
-        run_role<true, kF32, false>(I, s_info, wk);
+        run_role<true, kF32, false>(I, s_info, wk, -1);
         (void)n_work;
         return;
     }
     std::uint32_t staged = 0xFFFFFFFFu;
+    int burst = -1;  // help_push's answer for this step of the staged instance
     for (int wi = blockIdx.x; wi < n_work; wi += gridDim.x) {
         // Through L2 (never a cached line of an earlier chunk or engine):
         // the descriptors are rewritten by a host copy before every chunk.
@@ -1129,8 +1138,9 @@ __device__ __forceinline__ void step_body(const InstDev* __restrict__ insts,
                 asm volatile("griddepcontrol.launch_dependents;");
             }
             staged = wk.inst;
+            burst = -1;
         }
-        run_role<true, kF32, true>(I, s_info, wk);
+        burst = run_role<true, kF32, true>(I, s_info, wk, burst);
         __syncthreads();  // the role's shared arrays are free for the next item
     }
 }
@@ -1238,7 +1248,7 @@ __global__ void __launch_bounds__(kMaxBlock) chunk_kernel(const InstDev* __restr
             }
             if (threadIdx.x < 32) make_step_info(I, I.step0 + k, s_info);
             __syncthreads();
-            if (s_info.step < I.end_step) run_role<false, kF32, false>(I, s_info, wk);
+            if (s_info.step < I.end_step) run_role<false, kF32, false>(I, s_info, wk, -1);
         }
         if (k + 1 < steps && !grid_sync(gb, gridDim.x)) return;
     }
