@@ -488,14 +488,54 @@ __device__ __noinline__ double normal_clamped_at(std::uint64_t seed, std::uint64
     return normal_clamped(seed, stream);
 }
 
+// apply_arrivals (network.cpp:301-338) for one target: both short lists in
+// one batch, the counters cleared for the slot's next use, the excitatory
+// sum then the inhibitory one routed as add_synaptic_input does.
+__device__ __forceinline__ void apply_arrivals(const InstDev& I, std::uint32_t slot,
+                                               std::uint32_t c, std::size_t ts_ex,
+                                               std::size_t ts_in, std::uint32_t n_ex,
+                                               std::uint32_t n_in, double v0_ex, double& exc_in,
+                                               double& inh_in) {
+    ShortList lex{}, lin{};
+    if (n_ex > 1) lex = load_list(I.ring_ex, ts_ex);
+    if (n_in) lin = load_list(I.ring_in, ts_in);
+    if (n_ex) {
+        I.ring_ex.cnt[ts_ex] = 0;
+        // one arrival: 0.0 + v, the sum sum_arrivals forms for n = 1
+        const double ex =
+            n_ex == 1 ? 0.0 + v0_ex : sum_arrivals<false>(I.ring_ex, slot, c, n_ex, lex);
+        if (ex != 0.0) add_syn(ex, exc_in, inh_in);
+    }
+    if (n_in) {
+        I.ring_in.cnt[ts_in] = 0;
+        const double in = sum_arrivals<true>(I.ring_in, slot, c, n_in, lin);
+        if (in != 0.0) add_syn(-in, exc_in, inh_in);
+    }
+}
+
+struct SynIn {
+    double exc, inh;
+};
+
+__device__ __noinline__ SynIn arrivals_out_of_line(const InstDev& I, std::uint32_t slot,
+                                                   std::uint32_t c, std::size_t ts_ex,
+                                                   std::size_t ts_in, std::uint32_t n_ex,
+                                                   std::uint32_t n_in, double v0_ex) {
+    SynIn r{0.0, 0.0};
+    apply_arrivals(I, slot, c, ts_ex, ts_in, n_ex, n_in, v0_ex, r.exc, r.inh);
+    return r;
+}
+
 // --------------------------------------------------------------- roles
 
-// kWarpAppend: a warp's spikes take one atomic per warp (ballot and prefix
-// sums), which pays off when a step has many spiking warps (the wide form);
-// otherwise each spiking thread appends itself, the shortest chain for the
-// few spikes of a small network's step.  Either order of the spike records
-// gives the same rings (the arrivals are summed in bit order).
-template <bool kPdl, bool kWarpAppend>
+// kWide, the form for large steps: a warp's spikes take one atomic per warp
+// (ballot and prefix sums), which pays off when a step has many spiking
+// warps, and targets with several arrivals are summed out of line.
+// Otherwise each spiking thread appends itself, the shortest chain for the
+// few spikes of a small network's step, and the arrival lists stay inline.
+// Either order of the spike records gives the same rings (the arrivals are
+// summed in bit order).
+template <bool kPdl, bool kWide>
 __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     __shared__ std::uint32_t s_spk[kMaxBlock];
     __shared__ double s_val[2 * kMaxBlock];
@@ -508,17 +548,19 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
     // Written before the chunk started: read before waiting on the
     // previous step.
     double Vr = 0.0, bc = 0.0;
-    std::uint32_t r0 = 0, len0 = 0, len1 = 0;
+    std::uint32_t r0 = 0, len0 = 0, len1 = 0;  // out-edge rows (the wide form: on a spike)
     if (active) {
-        Vr = I.V_reset[c];
-        bc = I.b[c];
-        if (exc) {
-            r0 = I.exc_rs[c];
-            len0 = I.exc_rs[c + 1] - r0;
-            len1 = I.n2a_rs[c + 1] - I.n2a_rs[c];
-        } else {
-            r0 = I.inh_rs[c - I.NE];
-            len0 = I.inh_rs[c - I.NE + 1] - r0;
+        if (!kWide) {  // the wide form reads these where a reset needs them
+            Vr = I.V_reset[c];
+            bc = I.b[c];
+            if (exc) {
+                r0 = I.exc_rs[c];
+                len0 = I.exc_rs[c + 1] - r0;
+                len1 = I.n2a_rs[c + 1] - I.n2a_rs[c];
+            } else {
+                r0 = I.inh_rs[c - I.NE];
+                len0 = I.inh_rs[c - I.NE + 1] - r0;
+            }
         }
     }
     if (kPdl) grid_dep_wait();
@@ -547,8 +589,12 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
         double V = I.V[c], w = I.w[c], gex = I.gex[c], gin = I.gin[c];
         double dgex = I.dgex[c], dgin = I.dgin[c];
         int refr = I.refr[c];
+        // The source's STP state: prefetched with the state in the latency
+        // form; in the wide form read by a spiking thread only (one more
+        // round trip for a rare event, three fewer values live through the
+        // RK4).
         double sx = 1.0, su = 1.0, st = 0.0;
-        if (I.stp_on) {
+        if (!kWide && I.stp_on) {
             sx = I.stp_x[c];
             su = I.stp_u[c];
             st = I.stp_t[c];
@@ -578,22 +624,22 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
             }
         }
 
-        // apply_arrivals (network.cpp:301-338): both short lists in one batch.
-        ShortList lex{}, lin{};
-        if (n_ex > 1) lex = load_list(I.ring_ex, ts_ex);
-        if (n_in) lin = load_list(I.ring_in, ts_in);
         double exc_in = 0.0, inh_in = 0.0;
-        if (n_ex) {
-            I.ring_ex.cnt[ts_ex] = 0;
-            // one arrival: 0.0 + v, the sum sum_arrivals forms for n = 1
-            const double ex = n_ex == 1 ? 0.0 + v0_ex
-                                        : sum_arrivals<false>(I.ring_ex, slot, c, n_ex, lex);
-            if (ex != 0.0) add_syn(ex, exc_in, inh_in);
-        }
-        if (n_in) {
-            I.ring_in.cnt[ts_in] = 0;
-            const double in = sum_arrivals<true>(I.ring_in, slot, c, n_in, lin);
-            if (in != 0.0) add_syn(-in, exc_in, inh_in);
+        if constexpr (kWide) {
+            // Most targets of a large network see no arrival or a single
+            // excitatory one in a step; the rest go out of line, so the list
+            // registers are not live on the common path.
+            if (n_ex > 1 || n_in != 0u) {
+                const SynIn a = arrivals_out_of_line(I, slot, c, ts_ex, ts_in, n_ex, n_in, v0_ex);
+                exc_in = a.exc;
+                inh_in = a.inh;
+            } else if (n_ex) {
+                I.ring_ex.cnt[ts_ex] = 0;
+                const double ex = 0.0 + v0_ex;
+                if (ex != 0.0) add_syn(ex, exc_in, inh_in);
+            }
+        } else {
+            apply_arrivals(I, slot, c, ts_ex, ts_in, n_ex, n_in, v0_ex, exc_in, inh_in);
         }
         if (sic_due) {
             if (I.fused_sic)
@@ -620,7 +666,7 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
             const double gin1 = P.decay_in * (gin + h * dgin);
             const double dgin1 = P.decay_in * dgin;
             if (refr > 0) {
-                V = Vr;
+                V = kWide ? I.V_reset[c] : Vr;
                 const AdexRates r = adex<false>(P, V, w, gex, gin, Iext);
                 w += h * r.w;
             } else {
@@ -659,8 +705,8 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
             if (refr > 0) {
                 --refr;
             } else if (V >= P.V_peak) {
-                V = Vr;
-                w += bc;
+                V = kWide ? I.V_reset[c] : Vr;
+                w += kWide ? I.b[c] : bc;
                 refr = P.ref_steps;
                 spiked = true;
             }
@@ -676,6 +722,21 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
         double v0 = 0.0, v1 = 0.0;  // the values a spike's edges deliver
         std::uint32_t r1 = 0;
         if (spiked) {
+            if (kWide) {
+                if (I.stp_on) {
+                    sx = I.stp_x[c];
+                    su = I.stp_u[c];
+                    st = I.stp_t[c];
+                }
+                if (exc) {
+                    r0 = I.exc_rs[c];
+                    len0 = I.exc_rs[c + 1] - r0;
+                    len1 = I.n2a_rs[c + 1] - I.n2a_rs[c];
+                } else {
+                    r0 = I.inh_rs[c - I.NE];
+                    len0 = I.inh_rs[c - I.NE + 1] - r0;
+                }
+            }
             // Tsodyks-Markram update of this source (network.cpp:230-247); the
             // value its edges deliver is w*x*u per set.
             double x = 1.0, u = 1.0;
@@ -704,7 +765,7 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
             }
         }
 
-        if constexpr (!kWarpAppend) {
+        if constexpr (!kWide) {
             if (spiked) {
                 // One atomic reserves this spike's record and edge range.
                 if (I.deferred_push) {
@@ -739,8 +800,8 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
         const unsigned wbase = threadIdx.x & ~31u;
         const unsigned left = wk.count - wbase;  // > 0 for an active lane
         const unsigned act = left >= 32u ? 0xFFFFFFFFu : ((1u << left) - 1u);
-        const unsigned smask = kWarpAppend ? __ballot_sync(act, spiked) : 0u;  // syncs act
-        if (kWarpAppend && smask != 0u) {
+        const unsigned smask = kWide ? __ballot_sync(act, spiked) : 0u;  // syncs act
+        if (kWide && smask != 0u) {
             const unsigned rank = __popc(smask & ((1u << lane) - 1u));
             const int leader = __ffs(smask) - 1;
             const unsigned nspk = __popc(smask);
@@ -1067,7 +1128,7 @@ __device__ void sic_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     if ((threadIdx.x & 31) == 0 && edges) atomicAdd(I.counters + 1, edges);
 }
 
-template <bool kPdl, bool kF32, bool kWarpAppend>
+template <bool kPdl, bool kF32, bool kWide>
 __device__ __forceinline__ int run_role(const InstDev& I, const StepInfo& S, const Work& wk,
                                         int burst) {
     if (wk.role == kRolePush) {
@@ -1075,7 +1136,7 @@ __device__ __forceinline__ int run_role(const InstDev& I, const StepInfo& S, con
         return burst;
     }
     if (wk.role == kRoleNeuron) {
-        neuron_role<kPdl, kWarpAppend>(I, S, wk);
+        neuron_role<kPdl, kWide>(I, S, wk);
     } else if (wk.role == kRoleAstro) {
         astro_role<kPdl, kF32>(I, S, wk);
     } else {
