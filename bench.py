@@ -474,16 +474,8 @@ def bench_batched(sim_ms=5000.0, n_inst=64, autotune=True):
         plain_ms += ms
         plain_kernels += k
         net.close()
-    tuned = None
-    if autotune:
-        # Launch shapes ranked on a copy of the sweep run past its opening
-        # transient (the first ~0.2 s spike little and favour the latency
-        # form), over 1024 steps: long enough to rank chunk lengths.
-        t = Batch(models, record=rec, chunk_steps=128)
-        t.step(2048)
-        tuned = t.autotune(1024)
-        t.close()
-    b = Batch(models, record=rec, **(tuned or {"chunk_steps": 128}))
+    b = Batch(models, record=rec, chunk_steps=128)
+    tuned = b.autotune(1024) if autotune else None  # long enough to rank chunk lengths
     b.step(64)
     b.step(steps)
     bms, bk = b.last_timing()
