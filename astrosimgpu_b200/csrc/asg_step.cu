@@ -981,18 +981,26 @@ __device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
 }
 
 // A non-push block's share of a burst push, after its own role.
-// `burst` carries the answer across the items a block runs in one step of
-// one instance (-1: not known yet, else 0 or 1), so the spike count is read
-// once per block rather than once per item; the new answer is returned.
-__device__ __noinline__ int help_push(const InstDev& I, const StepInfo& S, const Work& wk,
-                                      int burst) {
+// A non-push block's share of a burst push (its rank among the helpers).
+__device__ __noinline__ void help_push_spikes(const InstDev& I, const StepInfo& S,
+                                              unsigned long long packed, std::uint32_t helper) {
+    push_spikes(I, S, packed, static_cast<std::uint32_t>(I.push_blocks) + helper,
+                static_cast<std::uint32_t>(I.push_blocks + I.push_helpers));
+}
+
+// After its own role, a block joins the push of step-1's spikes when that
+// push is a burst.  `burst` carries the answer across the items a block runs
+// in one step of one instance (-1: not known yet, else 0 or 1), so the spike
+// count is read once per block rather than once per item; the new answer is
+// returned.  Only a burst leaves the inline path.
+__device__ __forceinline__ int help_push(const InstDev& I, const StepInfo& S, const Work& wk,
+                                         int burst) {
     if (burst == 0 || !I.deferred_push || wk.helper == kNoHelper || S.step == 0 ||
         S.step >= I.end_step)
         return burst;
     const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev * kHeaderStride);
     if (!push_burst(I, packed)) return 0;
-    push_spikes(I, S, packed, static_cast<std::uint32_t>(I.push_blocks) + wk.helper,
-                static_cast<std::uint32_t>(I.push_blocks + I.push_helpers));
+    help_push_spikes(I, S, packed, wk.helper);
     return 1;
 }
 
