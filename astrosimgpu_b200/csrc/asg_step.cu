@@ -878,8 +878,19 @@ __device__ void neuron_role(const InstDev& I, const StepInfo& S, const Work& wk)
 constexpr int kPushBatch = 256;
 
 // The deferred push of the spikes of step-1 by participant `rank` of
-// `nranks` (each a block): edge x of the flat edge space goes to thread
-// x % (nranks * blockDim.x) of the participants.
+// `nranks` (each a block).  The spike list is cut into batches of
+// kPushBatch spikes.  kDealt (the wide form, whose bursts have ~10^4 helper
+// blocks and up to ~60 batches): the participants are dealt over the
+// batches -- with at least as many participants as batches, the Q
+// participants of batch b (ranks b, b + nbatch, ...) stage that batch once
+// and share its edges, edge x going to thread (x - first edge) %
+// (Q * blockDim.x) of them; with fewer, participant r pushes batches r,
+// r + nranks, ... alone -- so a participant stages only the batches it
+// pushes.  Otherwise (the latency form: tens of participants, one or two
+// batches) every participant stages every batch and edge x of the flat edge
+// space goes to thread x % (nranks * blockDim.x); the dealt form measured
+// 0.16 us slower per paper-sparse step there.
+template <bool kDealt>
 __device__ void push_spikes(const InstDev& I, const StepInfo& S, unsigned long long packed,
                             std::uint32_t rank, std::uint32_t nranks) {
     __shared__ std::uint32_t s_off[kPushBatch + 1], s_r0[kPushBatch], s_len0[kPushBatch],
@@ -887,11 +898,30 @@ __device__ void push_spikes(const InstDev& I, const StepInfo& S, unsigned long l
     __shared__ double s_v[2 * kPushBatch];
     const std::uint32_t n = static_cast<std::uint32_t>(packed >> 40);
     const std::uint32_t total = static_cast<std::uint32_t>(packed & 0xFFFFFFFFFFull);
-    const std::uint32_t stride = blockDim.x * nranks;
-    const std::uint32_t gtid = rank * blockDim.x + threadIdx.x;
+    if (n == 0) return;  // block-uniform
+    const std::uint32_t nbatch = (n + kPushBatch - 1) / kPushBatch;
     const std::uint32_t as_e = S.push_e, as_i = S.push_i;
     const std::size_t base = static_cast<std::size_t>(S.ls_prev) * I.N;
-    for (std::uint32_t b0 = 0; b0 < n; b0 += kPushBatch) {
+    // first batch, rank among the batch's participants, their number (no
+    // division in the common single-batch case)
+    std::uint32_t first = rank, q = 0, share = 1;
+    if (!kDealt) {  // every batch, all participants
+        first = 0;
+        q = rank;
+        share = nranks;
+    } else if (nbatch == 1) {
+        first = 0;
+        q = rank;
+        share = nranks;
+    } else if (nranks > nbatch) {
+        first = rank % nbatch;
+        q = rank / nbatch;
+        share = (nranks - 1 - first) / nbatch + 1;
+    }
+    const std::uint32_t stride = blockDim.x * share;
+    const std::uint32_t gtid = q * blockDim.x + threadIdx.x;
+    for (std::uint32_t bi = first; bi < nbatch; bi += kDealt ? nranks : 1u) {
+        const std::uint32_t b0 = bi * kPushBatch;
         const std::uint32_t nb = min(static_cast<std::uint32_t>(kPushBatch), n - b0);
         __syncthreads();
         for (std::uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
@@ -967,7 +997,7 @@ __device__ __forceinline__ bool push_burst(const InstDev& I, unsigned long long 
 // Deferred push of the spikes of step-1 by the PUSH blocks (joined by every
 // other block of the instance in a burst).  One thread also clears the list
 // slot the next step appends to.
-template <bool kPdl>
+template <bool kPdl, bool kWide>
 __device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     if (kPdl) grid_dep_wait();
     const std::int64_t step = S.step;
@@ -977,14 +1007,15 @@ __device__ void push_role(const InstDev& I, const StepInfo& S, const Work& wk) {
     const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev * kHeaderStride);
     const std::uint32_t nranks = static_cast<std::uint32_t>(I.push_blocks) +
                                  (push_burst(I, packed) ? I.push_helpers : 0u);
-    push_spikes(I, S, packed, wk.first, nranks);
+    push_spikes<kWide>(I, S, packed, wk.first, nranks);
 }
 
 // A non-push block's share of a burst push, after its own role.
 // A non-push block's share of a burst push (its rank among the helpers).
+template <bool kWide>
 __device__ __noinline__ void help_push_spikes(const InstDev& I, const StepInfo& S,
                                               unsigned long long packed, std::uint32_t helper) {
-    push_spikes(I, S, packed, static_cast<std::uint32_t>(I.push_blocks) + helper,
+    push_spikes<kWide>(I, S, packed, static_cast<std::uint32_t>(I.push_blocks) + helper,
                 static_cast<std::uint32_t>(I.push_blocks + I.push_helpers));
 }
 
@@ -993,6 +1024,7 @@ __device__ __noinline__ void help_push_spikes(const InstDev& I, const StepInfo& 
 // in one step of one instance (-1: not known yet, else 0 or 1), so the spike
 // count is read once per block rather than once per item; the new answer is
 // returned.  Only a burst leaves the inline path.
+template <bool kWide>
 __device__ __forceinline__ int help_push(const InstDev& I, const StepInfo& S, const Work& wk,
                                          int burst) {
     if (burst == 0 || !I.deferred_push || wk.helper == kNoHelper || S.step == 0 ||
@@ -1000,7 +1032,7 @@ __device__ __forceinline__ int help_push(const InstDev& I, const StepInfo& S, co
         return burst;
     const unsigned long long packed = __ldcg(I.spk_packed + S.ls_prev * kHeaderStride);
     if (!push_burst(I, packed)) return 0;
-    help_push_spikes(I, S, packed, wk.helper);
+    help_push_spikes<kWide>(I, S, packed, wk.helper);
     return 1;
 }
 
@@ -1140,7 +1172,7 @@ template <bool kPdl, bool kF32, bool kWide>
 __device__ __forceinline__ int run_role(const InstDev& I, const StepInfo& S, const Work& wk,
                                         int burst) {
     if (wk.role == kRolePush) {
-        push_role<kPdl>(I, S, wk);
+        push_role<kPdl, kWide>(I, S, wk);
         return burst;
     }
     if (wk.role == kRoleNeuron) {
@@ -1150,7 +1182,7 @@ __device__ __forceinline__ int run_role(const InstDev& I, const StepInfo& S, con
     } else {
         sic_role<kPdl>(I, S, wk);
     }
-    return help_push(I, S, wk, burst);
+    return help_push<kWide>(I, S, wk, burst);
 }
 
 // One step of every resident instance (the body of both kernel forms below).
