@@ -426,7 +426,7 @@ struct AstroEngine {
     // Events keep each range's order: input copy -> update -> Ca copy, and
     // the next step's input copy and update after this step's update and Ca
     // copy of the same range.
-    static constexpr int kMaxPieces = 16;
+    static constexpr int kMaxPieces = 8;
     static constexpr std::int64_t kPieceCells = 1 << 18;
     cudaStream_t h2d = nullptr, d2h = nullptr;
     cudaEvent_t ev_in[kMaxPieces] = {}, ev_k[kMaxPieces] = {}, ev_out[kMaxPieces] = {};

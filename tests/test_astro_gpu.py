@@ -67,7 +67,7 @@ def test_drop_in_backend_per_cell_params_and_input():
 
 
 def test_drop_in_backend_pipelined_cell_ranges():
-    """Large handles copy and update in up to sixteen cell ranges whose copies
+    """Large handles copy and update in up to eight cell ranges whose copies
     overlap the updates; the result is the oracle's, bit for bit, including
     at range boundaries, on consecutive steps and when the caller reuses one
     input buffer."""
