@@ -173,6 +173,7 @@ void Server::retire(Request& r, int status) {
 // stepping the resident requests.  Prepared requests are staged; the loop
 // joins them at its next chunk boundary.
 void Server::admit_loop() {
+    cudaSetDevice(eng->cfg.device);  // this thread's calls go to the server's GPU
     std::unique_lock<std::mutex> lk(mu);
     while (!stop) {
         if (queue.empty()) {
@@ -244,6 +245,7 @@ void Server::admit_loop() {
 // those that reached their last step.  Requests join and leave only at chunk
 // boundaries, so a request's arithmetic is the same alone and in any mix.
 void Server::loop() {
+    cudaSetDevice(eng->cfg.device);  // this thread's calls go to the server's GPU
     std::unique_lock<std::mutex> lk(mu);
     while (!stop) {
         for (auto& kv : reqs) {
